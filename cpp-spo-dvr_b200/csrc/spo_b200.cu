@@ -1,0 +1,749 @@
+// Host side of the B200 split-operator backend: the handle, the table set-up and the C ABI of
+// include/spo_b200.h. One handle = one wave packet resident in HBM, one CUDA stream.
+//
+// One sub-step of the reference's schedule (src/propagation/split_operator.cpp:17-21,
+// split_operator_schedule.cpp:7-13) is, on the device:
+//   specular grid   3 axis passes: r forward | Z forward * factor * inverse | r inverse (+ W factors)
+//   T_Z             1 axis pass over psi (Z forward * exp(-i T_Z dt) * inverse)
+//   T_r             1 axis pass over psi (r forward * exp(-i T_r dt) * inverse)
+//   T_xy (+ W gas)  1 pass over psi, 2D (x, y) FFT per (Z, r) point, gas-phase W fused
+//   W interaction   1 pass over the interaction region (theta contraction, phi FFTs, exp(iA))
+// T_Z and T_r are applied separably: the reference's 2D factor zr_kinetic is the product
+// z_kinetic * r_kinetic (src/propagation/propagation_tables.cpp:157-162), so
+// F_zr^-1 (z r) F_zr = (F_Z^-1 z F_Z)(F_r^-1 r F_r) exactly, up to rounding.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/spo_b200.h"
+#include "spo_kernels.cuh"
+
+namespace {
+
+using cplx = std::complex<double>;
+
+thread_local std::string g_create_error;
+
+struct SpoError : std::runtime_error {
+  int code;
+  SpoError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) throw SpoError(SPO_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) throw SpoError(SPO_ERR_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void require(bool ok, const std::string& what) {
+  if (!ok) throw SpoError(SPO_ERR_INVALID, what);
+}
+
+// Radices of a valid FFT length (2^h 3^i 5^j 7^k 11^m), fours first.
+spo::FftPlan make_plan(int n) {
+  spo::FftPlan p{};
+  p.n = n;
+  int m = n;
+  auto push = [&](int r) {
+    require(p.n_stages < spo::kMaxStages, "FFT length " + std::to_string(n) + " has too many factors");
+    p.radix[p.n_stages++] = r;
+  };
+  while (m % 4 == 0) push(4), m /= 4;
+  for (const int r : {2, 3, 5, 7, 11})
+    while (m % r == 0) push(r), m /= r;
+  require(m == 1, "FFT length " + std::to_string(n) + " is not 2^h 3^i 5^j 7^k 11^m");
+  return p;
+}
+
+// exp(-2 pi i k / n), k < n, in FP64 (exact on the axes).
+std::vector<cplx> twiddles(int n) {
+  std::vector<cplx> t(n);
+  for (int k = 0; k < n; ++k) {
+    if (k == 0) t[k] = {1, 0};
+    else if (4 * k == n) t[k] = {0, -1};
+    else if (2 * k == n) t[k] = {-1, 0};
+    else if (4 * k == 3 * n) t[k] = {0, 1};
+    else {
+      const double a = 2.0 * M_PI * k / n;
+      t[k] = {std::cos(a), -std::sin(a)};
+    }
+  }
+  return t;
+}
+
+std::vector<cplx> complex_array(const double* p, std::size_t n, const char* name) {
+  require(p != nullptr, std::string("descriptor array ") + name + " is null");
+  std::vector<cplx> v(n);
+  for (std::size_t i = 0; i < n; ++i) v[i] = {p[2 * i], p[2 * i + 1]};
+  return v;
+}
+std::vector<double> real_array(const double* p, std::size_t n, const char* name) {
+  require(p != nullptr, std::string("descriptor array ") + name + " is null");
+  return std::vector<double>(p, p + n);
+}
+std::vector<int> int_array(const int* p, std::size_t n, const char* name) {
+  require(p != nullptr, std::string("descriptor array ") + name + " is null");
+  return std::vector<int>(p, p + n);
+}
+
+// Owned device allocations of a handle.
+class DeviceArena {
+ public:
+  ~DeviceArena() {
+    for (void* p : ptrs_) cudaFree(p);
+  }
+  void* alloc(std::size_t bytes) {
+    void* p = nullptr;
+    check_cuda(cudaMalloc(&p, std::max<std::size_t>(bytes, 16)), "cudaMalloc");
+    ptrs_.push_back(p);
+    bytes_ += bytes;
+    return p;
+  }
+  void release(void* p, std::size_t bytes) {
+    auto it = std::find(ptrs_.begin(), ptrs_.end(), p);
+    if (it == ptrs_.end()) return;
+    cudaFree(p);
+    ptrs_.erase(it);
+    bytes_ -= bytes;
+  }
+  unsigned long long bytes() const { return bytes_; }
+
+ private:
+  std::vector<void*> ptrs_;
+  unsigned long long bytes_ = 0;
+};
+
+struct Sizes {
+  int n_rot, nx, ny, nr, nz, nzp, nzs, nt, nphi, i0, ra, rb, spa, n_rep, n_ops, n_blocks, mj_max;
+  double dt;
+  long long n_xy() const { return static_cast<long long>(nx) * ny; }
+  long long n_zr() const { return static_cast<long long>(nz) * nr; }
+  long long n_psi() const { return n_xy() * n_zr() * n_rot; }
+  long long n_chi() const { return static_cast<long long>(nzs) * nr; }
+  long long n_expia() const { return static_cast<long long>(nzp) * nr * n_rep * nt * nphi; }
+};
+
+class StepBase {
+ public:
+  virtual ~StepBase() = default;
+  virtual void propagate_analysis_step() = 0;
+  virtual void upload(const double* psi, const double* chi) = 0;
+  virtual void download(double* psi, double* chi) = 0;
+  virtual void z_plane(int iz, double* out) = 0;
+  virtual void block_densities(double* out) = 0;
+  virtual void site_column(int ixy, double* out) = 0;
+  virtual void apply_stage(int stage, bool half) = 0;
+  virtual unsigned long long bytes() const = 0;
+  virtual int launches() const = 0;
+};
+
+template <typename T>
+class Step final : public StepBase {
+  using V = spo::Vec<T>;
+
+ public:
+  Step(const spo_desc& d, const Sizes& s, cudaStream_t stream) : s_(s), stream_(stream) { build(d); }
+
+  void propagate_analysis_step() override {
+    launches_ = 0;
+    const int n = s_.spa;
+    for (int k = 0; k <= n; ++k) {
+      const bool half = k == 0 || k == n;  // T(dt/2) V, (T V) n-1 times, T(dt/2)
+      const bool kinetic_only = k == n;
+      sub_step(half, kinetic_only);
+    }
+    check_cuda(cudaGetLastError(), "propagate_analysis_step launch");
+    check_cuda(cudaStreamSynchronize(stream_), "propagate_analysis_step");
+  }
+
+  void upload(const double* psi, const double* chi) override {
+    if (psi) copy_in(psi, psi_, s_.n_psi());
+    if (chi) copy_in(chi, chi_, s_.n_chi());
+    check_cuda(cudaStreamSynchronize(stream_), "upload");
+  }
+
+  void download(double* psi, double* chi) override {
+    if (psi) copy_out(psi_, psi, s_.n_psi());
+    if (chi) copy_out(chi_, chi, s_.n_chi());
+    check_cuda(cudaStreamSynchronize(stream_), "download");
+  }
+
+  void z_plane(int iz, double* out) override {
+    require(iz >= 0 && iz < s_.nz, "z_plane: iz out of range");
+    const long long plane = s_.n_xy() * s_.nr * s_.n_rot;
+    copy_out(psi_ + plane * iz, out, plane);
+    check_cuda(cudaStreamSynchronize(stream_), "z_plane");
+  }
+
+  void block_densities(double* out) override {
+    spo::block_density_kernel<T><<<static_cast<unsigned>(s_.n_zr()), 256, 0, stream_>>>(
+        psi_, s_.n_xy() * s_.n_rot, densities_);
+    check_cuda(cudaGetLastError(), "block_densities launch");
+    check_cuda(cudaMemcpyAsync(out, densities_, sizeof(double) * s_.n_zr(), cudaMemcpyDeviceToHost, stream_),
+               "block_densities copy");
+    check_cuda(cudaStreamSynchronize(stream_), "block_densities");
+  }
+
+  void site_column(int ixy, double* out) override {
+    require(ixy >= 0 && ixy < s_.n_xy(), "site_column: ixy out of range");
+    const long long n = s_.n_zr() * s_.n_rot;
+    spo::site_column_kernel<T><<<592, 256, 0, stream_>>>(psi_, staging_, s_.n_rot, static_cast<int>(s_.n_xy()),
+                                                         s_.n_zr(), ixy);
+    check_cuda(cudaGetLastError(), "site_column launch");
+    // staging_ holds staging_elems_ complex values; the column is n_zr*n_rot <= that (checked at build).
+    check_cuda(cudaMemcpyAsync(out, staging_, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream_),
+               "site_column copy");
+    check_cuda(cudaStreamSynchronize(stream_), "site_column");
+  }
+
+  void apply_stage(int stage, bool half) override {
+    launches_ = 0;
+    switch (stage) {
+      case SPO_STAGE_SPECULAR: specular(half, false); break;
+      case SPO_STAGE_SPECULAR_KINETIC: specular(half, true); break;
+      case SPO_STAGE_ZR: kinetic_zr(half); break;
+      case SPO_STAGE_XY: kinetic_xy(half, false); break;
+      case SPO_STAGE_POTENTIAL:
+        gas_phase();
+        interaction();
+        break;
+      default: require(false, "unknown stage");
+    }
+    check_cuda(cudaGetLastError(), "apply_stage launch");
+    check_cuda(cudaStreamSynchronize(stream_), "apply_stage");
+  }
+
+  unsigned long long bytes() const override { return arena_.bytes(); }
+  int launches() const override { return launches_; }
+
+ private:
+  // ------------------------------------------------------------------ one sub-step
+  void sub_step(bool half, bool kinetic_only) {
+    specular(half, kinetic_only);
+    kinetic_zr(half);
+    kinetic_xy(half, !kinetic_only);  // the gas-phase potential step rides along
+    if (!kinetic_only) interaction();
+  }
+
+  // Specular grid: r forward, Z forward * factor * inverse, r inverse (* W factors).
+  void specular(bool half, bool kinetic_only) {
+    axis(chi_, /*outer*/ s_.nzs, plan_r_, tw_r_, /*inner*/ 1, nullptr, spo::kNoFactor, spo::kFwdFactor, nullptr);
+    axis(chi_, 1, plan_zs_, tw_zs_, s_.nr, half ? spec_half_ : spec_full_, spo::kFactorAxisInner,
+         spo::kFwdFactorInv, nullptr);
+    axis(chi_, s_.nzs, plan_r_, tw_r_, 1, nullptr, spo::kNoFactor, spo::kFactorInv, kinetic_only ? nullptr : spec_w_);
+  }
+
+  // T_Z and T_r of the scattering wave.
+  void kinetic_zr(bool half) {
+    axis(psi_, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, spo::kFactorAxis,
+         spo::kFwdFactorInv, nullptr);
+    axis(psi_, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, spo::kFactorAxis,
+         spo::kFwdFactorInv, nullptr);
+  }
+
+  // T_xy, optionally with the gas-phase potential step fused.
+  void kinetic_xy(bool half, bool with_gas) {
+    spo::XyArgs<T> x{};
+    x.psi = psi_;
+    x.n_rot = s_.n_rot;
+    x.nx = s_.nx;
+    x.ny = s_.ny;
+    x.px = plan_x_;
+    x.py = plan_y_;
+    x.twx = tw_x_;
+    x.twy = tw_y_;
+    x.factor = half ? xyk_half_ : xyk_full_;
+    x.shift_f = shift_f_;
+    x.shift_b = shift_b_;
+    x.tb = xy_tb_;
+    x.apply_gas = with_gas ? 1 : 0;
+    x.izr_gas_first = static_cast<long long>(s_.nzp) * s_.nr;
+    x.nr = s_.nr;
+    x.opt_z = opt_z_;
+    x.gas_step = gas_step_;
+    const dim3 xg((s_.n_rot + xy_tb_ - 1) / xy_tb_, static_cast<unsigned>(s_.n_zr()));
+    spo::xy_pass_kernel<T><<<xg, 256, xy_smem_, stream_>>>(x);
+    ++launches_;
+  }
+
+  void gas_phase() {
+    const long long first = static_cast<long long>(s_.nzp) * s_.nr;
+    if (first >= s_.n_zr()) return;
+    spo::gas_phase_kernel<T><<<1184, 256, 0, stream_>>>(psi_, first, s_.n_zr(), s_.n_rot, static_cast<int>(s_.n_xy()),
+                                                        s_.nr, opt_z_, gas_step_);
+    ++launches_;
+  }
+
+  void interaction() {
+    if (s_.nzp == 0) return;
+    spo::potential_kernel<T><<<static_cast<unsigned>(s_.nzp) * s_.nr, 256, pot_smem_, stream_>>>(pot_);
+    ++launches_;
+  }
+
+  void axis(V* data, long long outer, const spo::FftPlan& plan, const V* tw, long long inner, const V* factor,
+            int factor_mode, int dir, const V* post) {
+    spo::AxisArgs<T> a{};
+    a.data = data;
+    a.inner = inner;
+    a.plan = plan;
+    a.tw = tw;
+    a.factor = factor;
+    a.factor_mode = factor_mode;
+    a.dir = dir;
+    a.post = post;
+    a.tb = axis_tile(plan.n, inner);
+    const std::size_t smem = sizeof(V) * (2 * static_cast<std::size_t>(plan.n) * a.tb + plan.n);
+    const dim3 grid(static_cast<unsigned>((inner + a.tb - 1) / a.tb), static_cast<unsigned>(outer));
+    spo::axis_pass_kernel<T><<<grid, 256, smem, stream_>>>(a);
+    ++launches_;
+  }
+
+  // Inner elements per axis-pass tile: a power of two up to 64 (coalesced rows of tb * sizeof(V)
+  // bytes), at most ~64 KiB of shared memory for the two ping-pong buffers, at most `inner`.
+  static int axis_tile(int n, long long inner) {
+    int tb = 64;
+    while (tb > 1 && 2ull * n * tb * sizeof(V) > (64u << 10)) tb /= 2;
+    while (tb > 1 && tb / 2 >= inner) tb /= 2;
+    return tb;
+  }
+
+  // ------------------------------------------------------------------ set-up
+  template <typename U>
+  U* dev(std::size_t n) {
+    return static_cast<U*>(arena_.alloc(sizeof(U) * n));
+  }
+
+  V* upload_complex(const std::vector<cplx>& v) {
+    std::vector<V> h(v.size());
+    for (std::size_t i = 0; i < v.size(); ++i) {
+      h[i].x = static_cast<T>(v[i].real());
+      h[i].y = static_cast<T>(v[i].imag());
+    }
+    V* d = dev<V>(v.size());
+    check_cuda(cudaMemcpy(d, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice), "upload table");
+    return d;
+  }
+  T* upload_real(const std::vector<double>& v) {
+    std::vector<T> h(v.begin(), v.end());
+    T* d = dev<T>(v.size());
+    check_cuda(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice), "upload table");
+    return d;
+  }
+  int* upload_int(const std::vector<int>& v) {
+    int* d = dev<int>(v.size());
+    check_cuda(cudaMemcpy(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice), "upload table");
+    return d;
+  }
+
+  void build(const spo_desc& d) {
+    const Sizes& s = s_;
+    const long long nxy = s.n_xy();
+    plan_z_ = make_plan(s.nz);
+    plan_r_ = make_plan(s.nr);
+    plan_x_ = make_plan(s.nx);
+    plan_y_ = make_plan(s.ny);
+    plan_zs_ = make_plan(s.nzs);
+    plan_phi_ = make_plan(s.nphi);
+    tw_z_ = upload_complex(twiddles(s.nz));
+    tw_r_ = upload_complex(twiddles(s.nr));
+    tw_x_ = upload_complex(twiddles(s.nx));
+    tw_y_ = upload_complex(twiddles(s.ny));
+    tw_zs_ = upload_complex(twiddles(s.nzs));
+    tw_phi_ = upload_complex(twiddles(s.nphi));
+
+    // Kinetic factors with the FFT scales folded in (the reference applies the forward scale after
+    // the forward transform and 1/(n*scale) after the inverse: the product of both is 1/n per axis).
+    auto scaled = [](std::vector<cplx> v, double f) {
+      for (auto& x : v) x *= f;
+      return v;
+    };
+    zk_full_ = upload_complex(scaled(complex_array(d.z_kinetic_full, s.nz, "z_kinetic_full"), 1.0 / s.nz));
+    zk_half_ = upload_complex(scaled(complex_array(d.z_kinetic_half, s.nz, "z_kinetic_half"), 1.0 / s.nz));
+    rk_full_ = upload_complex(scaled(complex_array(d.r_kinetic_full, s.nr, "r_kinetic_full"), 1.0 / s.nr));
+    rk_half_ = upload_complex(scaled(complex_array(d.r_kinetic_half, s.nr, "r_kinetic_half"), 1.0 / s.nr));
+    const double sx = s.nx > 1 ? d.fft_scale_x : 1.0;
+    const double sy = s.ny > 1 ? d.fft_scale_y : 1.0;
+    const double xy_scale = (sx * sy) * ((1.0 / (s.nx * sx)) * (1.0 / (s.ny * sy)));
+    xyk_full_ = upload_complex(scaled(complex_array(d.xy_kinetic_full, nxy, "xy_kinetic_full"), xy_scale));
+    xyk_half_ = upload_complex(scaled(complex_array(d.xy_kinetic_half, nxy, "xy_kinetic_half"), xy_scale));
+    const double sz = d.fft_scale_z, sr = d.fft_scale_r;
+    const double spec_scale = (sz * sr) * ((1.0 / (s.nzs * sz)) * (1.0 / (s.nr * sr)));
+    spec_full_ = upload_complex(scaled(complex_array(d.specular_kinetic_full, s.n_chi(), "specular_kinetic_full"), spec_scale));
+    spec_half_ = upload_complex(scaled(complex_array(d.specular_kinetic_half, s.n_chi(), "specular_kinetic_half"), spec_scale));
+
+    // Potential-step factors (src/propagation/potential_operator.cpp:15-26) and the specular grid's
+    // W factors (src/propagation/specular_operator.cpp:11-19, 58-71), merged in FP64.
+    const std::vector<cplx> rot = complex_array(d.rotation_half, static_cast<std::size_t>(s.n_rot) * s.nr, "rotation_half");
+    const std::vector<double> opt_r = real_array(d.r_optical, s.nr, "r_optical");
+    const std::vector<double> opt_z = real_array(d.z_optical, s.nz, "z_optical");
+    const std::vector<double> opt_zs = real_array(d.z_specular_optical, s.nzs, "z_specular_optical");
+    const std::vector<cplx> gas = complex_array(d.gas_phase, s.nr, "gas_phase");
+    std::vector<cplx> before(rot.size()), gas_step(rot.size());
+    for (int ir = 0; ir < s.nr; ++ir)
+      for (int irot = 0; irot < s.n_rot; ++irot) {
+        const cplx r = rot[irot + static_cast<std::size_t>(s.n_rot) * ir];
+        const double o = s.nr != 1 ? opt_r[ir] : 1.0;
+        before[static_cast<std::size_t>(ir) * s.n_rot + irot] = o * r;
+        gas_step[static_cast<std::size_t>(ir) * s.n_rot + irot] = o * r * gas[ir] * r;
+      }
+    std::vector<cplx> spec_w(s.n_chi());
+    for (int iz = 0; iz < s.nzs; ++iz)
+      for (int ir = 0; ir < s.nr; ++ir) {
+        const cplx r = rot[s.i0 + static_cast<std::size_t>(s.n_rot) * ir];
+        cplx f = iz >= s.nzp ? r * gas[ir] * r : cplx(1.0, 0.0);
+        f *= opt_zs[iz];
+        if (s.nr != 1 && ir >= s.ra && ir <= s.rb) f *= opt_r[ir];
+        spec_w[ir + static_cast<std::size_t>(s.nr) * iz] = f;
+      }
+    rot_half_ = upload_complex([&] {
+      std::vector<cplx> v(rot.size());
+      for (int ir = 0; ir < s.nr; ++ir)
+        for (int irot = 0; irot < s.n_rot; ++irot)
+          v[static_cast<std::size_t>(ir) * s.n_rot + irot] = rot[irot + static_cast<std::size_t>(s.n_rot) * ir];
+      return v;
+    }());
+    before_ = upload_complex(before);
+    gas_step_ = upload_complex(gas_step);
+    spec_w_ = upload_complex(spec_w);
+    opt_z_ = upload_real(opt_z);
+
+    const std::vector<cplx> shf = complex_array(d.shift_forward, nxy, "shift_forward");
+    const bool shift = std::any_of(shf.begin(), shf.end(), [](const cplx& c) { return c.real() != 1.0 || c.imag() != 0.0; });
+    if (shift) {
+      shift_f_ = upload_complex(shf);
+      shift_b_ = upload_complex(complex_array(d.shift_backward, nxy, "shift_backward"));
+    }
+    const V* sp2sc = upload_complex(complex_array(d.specular_to_scattering, nxy, "specular_to_scattering"));
+    const V* sc2sp = upload_complex(complex_array(d.scattering_to_specular, nxy, "scattering_to_specular"));
+
+    // Angular transform tables.
+    const std::vector<int> first = int_array(d.mj_fbr_first, s.n_blocks, "mj_fbr_first");
+    const std::vector<int> size = int_array(d.mj_fbr_size, s.n_blocks, "mj_fbr_size");
+    const std::vector<int> slot = int_array(d.mj_phi_slot, s.n_blocks, "mj_phi_slot");
+    std::vector<int> offset(s.n_blocks), irot_block(s.n_rot, -1);
+    int off = 0, total_j = 0;
+    for (int b = 0; b < s.n_blocks; ++b) {
+      offset[b] = off;
+      off += s.nt * size[b];
+      total_j += size[b];
+      const int m = b - s.mj_max;
+      require(slot[b] == (m >= 0 ? m : s.nphi + m), "mj_phi_slot does not follow the mJ order");
+      for (int j = 0; j < size[b]; ++j) {
+        require(first[b] + j >= 0 && first[b] + j < s.n_rot, "mj block outside the rotational basis");
+        irot_block[first[b] + j] = b;
+      }
+    }
+    require(total_j == s.n_rot, "mj blocks do not cover the rotational basis");
+    const std::vector<double> legendre = real_array(d.legendre, static_cast<std::size_t>(off), "legendre");
+
+    // Symmetry maps, expanded to one phi map per (x, y) point.
+    const std::vector<int> rep = int_array(d.representative_of, nxy, "representative_of");
+    const std::vector<int> op = int_array(d.operation_of, nxy, "operation_of");
+    const std::vector<int> phi_index = int_array(d.phi_index, static_cast<std::size_t>(s.n_ops) * s.nphi, "phi_index");
+    std::vector<int> phi_map(nxy * s.nphi);
+    for (long long ixy = 0; ixy < nxy; ++ixy) {
+      require(rep[ixy] >= 0 && rep[ixy] < s.n_rep, "representative_of out of range");
+      require(op[ixy] >= 0 && op[ixy] < s.n_ops, "operation_of out of range");
+      for (int p = 0; p < s.nphi; ++p) {
+        const int q = phi_index[static_cast<std::size_t>(op[ixy]) * s.nphi + p];
+        require(q >= 0 && q < s.nphi, "phi_index out of range");
+        phi_map[ixy * s.nphi + p] = q;
+      }
+    }
+
+    // State.
+    psi_ = dev<V>(s.n_psi());
+    check_cuda(cudaMemsetAsync(psi_, 0, sizeof(V) * s.n_psi(), stream_), "zero psi");
+    chi_ = dev<V>(s.n_chi());
+    densities_ = dev<double>(s.n_zr());
+    staging_elems_ = std::max<long long>(s.n_zr() * s.n_rot, 4ll << 20);
+    staging_ = dev<double2>(staging_elems_);
+    require(d.chi_initial != nullptr, "chi_initial is null");
+    upload(nullptr, d.chi_initial);
+
+    // exp(i A) on the device in FP64, chunk by chunk through the staging buffer.
+    const long long n_e = s.n_expia();
+    require(d.potential != nullptr || n_e == 0, "potential is null");
+    expia_ = dev<V>(std::max<long long>(n_e, 1));
+    double* vstage = reinterpret_cast<double*>(staging_);
+    const long long chunk = 2 * staging_elems_;
+    for (long long i = 0; i < n_e; i += chunk) {
+      const long long m = std::min(chunk, n_e - i);
+      check_cuda(cudaMemcpyAsync(vstage, d.potential + i, sizeof(double) * m, cudaMemcpyHostToDevice, stream_),
+                 "upload potential");
+      spo::exp_potential_kernel<T><<<1184, 256, 0, stream_>>>(vstage, expia_ + i, m, s.dt);
+      check_cuda(cudaGetLastError(), "exp_potential launch");
+      check_cuda(cudaStreamSynchronize(stream_), "exp_potential");
+    }
+
+    // Launch shapes and shared memory.
+    int smem_optin = 0, dev_id = 0;
+    check_cuda(cudaGetDevice(&dev_id), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev_id), "smem attribute");
+    check_cuda(cudaFuncSetAttribute(spo::axis_pass_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
+               "axis smem");
+    for (const int n : {s.nz, s.nr, s.nzs}) require(2ull * n * sizeof(V) + n * sizeof(V) <= static_cast<unsigned>(smem_optin),
+                                                     "FFT length too long for shared memory");
+    xy_tb_ = 1;
+    while (xy_tb_ < 32 && xy_tb_ < s.n_rot && 2ull * nxy * (2 * xy_tb_) * sizeof(V) <= (96u << 10)) xy_tb_ *= 2;
+    xy_smem_ = sizeof(V) * (2 * nxy * xy_tb_ + s.nx + s.ny);
+    require(xy_smem_ <= static_cast<std::size_t>(smem_optin), "nx*ny too large for the xy pass");
+    check_cuda(cudaFuncSetAttribute(spo::xy_pass_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
+               "xy smem");
+
+    const int ld = s.nphi + 1;
+    auto pot_bytes = [&](int cb) {
+      return sizeof(V) * (static_cast<std::size_t>(cb) * s.n_rot + 2ull * cb * s.nt * ld + s.nphi + nxy + 32) +
+             sizeof(T) * static_cast<std::size_t>(s.nt) * s.n_rot;
+    };
+    int cb = 1;
+    while (cb < 16 && cb < nxy && pot_bytes(cb + 1) <= std::min<std::size_t>(smem_optin, 112u << 10)) ++cb;
+    require(pot_bytes(cb) <= static_cast<std::size_t>(smem_optin), "angular grid too large for the potential step");
+    pot_smem_ = pot_bytes(cb);
+    check_cuda(cudaFuncSetAttribute(spo::potential_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
+               "potential smem");
+    pot_.psi = psi_;
+    pot_.chi = chi_;
+    pot_.n_rot = s.n_rot;
+    pot_.n_xy = static_cast<int>(nxy);
+    pot_.nr = s.nr;
+    pot_.n_theta = s.nt;
+    pot_.n_phi = s.nphi;
+    pot_.ld = ld;
+    pot_.n_blocks = s.n_blocks;
+    pot_.mj_max = s.mj_max;
+    pot_.initial_channel = s.i0;
+    pot_.n_rep = s.n_rep;
+    pot_.cb = cb;
+    pot_.pphi = plan_phi_;
+    pot_.twphi = tw_phi_;
+    pot_.legendre = upload_real(legendre);
+    pot_.block_first = upload_int(first);
+    pot_.block_size = upload_int(size);
+    pot_.block_slot = upload_int(slot);
+    pot_.block_offset = upload_int(offset);
+    pot_.irot_block = upload_int(irot_block);
+    pot_.opt_z = opt_z_;
+    pot_.before = before_;
+    pot_.rot_half = rot_half_;
+    pot_.sp2sc = sp2sc;
+    pot_.sc2sp = sc2sp;
+    pot_.expia = expia_;
+    pot_.rep_of = upload_int(rep);
+    pot_.phi_map = upload_int(phi_map);
+    check_cuda(cudaStreamSynchronize(stream_), "set-up");
+  }
+
+  // Host FP64 complex -> device T, through the staging buffer.
+  void copy_in(const double* src, V* dst, long long n) {
+    for (long long i = 0; i < n; i += staging_elems_) {
+      const long long m = std::min(staging_elems_, n - i);
+      if constexpr (std::is_same_v<T, double>) {
+        check_cuda(cudaMemcpyAsync(dst + i, src + 2 * i, sizeof(double2) * m, cudaMemcpyHostToDevice, stream_), "upload");
+      } else {
+        check_cuda(cudaMemcpyAsync(staging_, src + 2 * i, sizeof(double2) * m, cudaMemcpyHostToDevice, stream_), "upload");
+        spo::convert_kernel<T, double><<<1184, 256, 0, stream_>>>(staging_, dst + i, m);
+        check_cuda(cudaGetLastError(), "convert launch");
+        check_cuda(cudaStreamSynchronize(stream_), "upload");
+      }
+    }
+  }
+  void copy_out(const V* src, double* dst, long long n) {
+    for (long long i = 0; i < n; i += staging_elems_) {
+      const long long m = std::min(staging_elems_, n - i);
+      if constexpr (std::is_same_v<T, double>) {
+        check_cuda(cudaMemcpyAsync(dst + 2 * i, src + i, sizeof(double2) * m, cudaMemcpyDeviceToHost, stream_), "download");
+      } else {
+        spo::convert_kernel<double, T><<<1184, 256, 0, stream_>>>(src + i, staging_, m);
+        check_cuda(cudaGetLastError(), "convert launch");
+        check_cuda(cudaMemcpyAsync(dst + 2 * i, staging_, sizeof(double2) * m, cudaMemcpyDeviceToHost, stream_), "download");
+        check_cuda(cudaStreamSynchronize(stream_), "download");
+      }
+    }
+  }
+
+  Sizes s_;
+  cudaStream_t stream_;
+  DeviceArena arena_;
+  int launches_ = 0;
+  spo::FftPlan plan_z_{}, plan_r_{}, plan_x_{}, plan_y_{}, plan_zs_{}, plan_phi_{};
+  V *tw_z_ = nullptr, *tw_r_ = nullptr, *tw_x_ = nullptr, *tw_y_ = nullptr, *tw_zs_ = nullptr, *tw_phi_ = nullptr;
+  V *zk_full_ = nullptr, *zk_half_ = nullptr, *rk_full_ = nullptr, *rk_half_ = nullptr;
+  V *xyk_full_ = nullptr, *xyk_half_ = nullptr, *spec_full_ = nullptr, *spec_half_ = nullptr;
+  V *rot_half_ = nullptr, *before_ = nullptr, *gas_step_ = nullptr, *spec_w_ = nullptr;
+  V *shift_f_ = nullptr, *shift_b_ = nullptr;
+  T* opt_z_ = nullptr;
+  V *psi_ = nullptr, *chi_ = nullptr, *expia_ = nullptr;
+  double* densities_ = nullptr;
+  double2* staging_ = nullptr;
+  long long staging_elems_ = 0;
+  int xy_tb_ = 1;
+  std::size_t xy_smem_ = 0, pot_smem_ = 0;
+  spo::PotArgs<T> pot_{};
+};
+
+Sizes sizes_of(const spo_desc& d) {
+  Sizes s{};
+  s.n_rot = d.n_rot;
+  s.nx = d.nx;
+  s.ny = d.ny;
+  s.nr = d.nr;
+  s.nz = d.nz;
+  s.nzp = d.nz_potential;
+  s.nzs = d.nz_specular;
+  s.nt = d.n_theta;
+  s.nphi = d.n_phi;
+  s.i0 = d.initial_channel;
+  s.ra = d.r_absorber_first;
+  s.rb = d.r_absorber_last;
+  s.spa = d.steps_per_analysis;
+  s.n_rep = d.n_rep;
+  s.n_ops = d.n_ops;
+  s.n_blocks = d.n_mj_blocks;
+  s.mj_max = (d.n_mj_blocks - 1) / 2;
+  s.dt = d.time_step;
+  require(s.n_rot > 0 && s.nx > 0 && s.ny > 0 && s.nr > 1 && s.nz > 0 && s.nzs > 0, "grid sizes must be positive (nR >= 2)");
+  require(s.nzp >= 0 && s.nzp <= s.nz && s.nzp <= s.nzs, "nz_potential out of range");
+  require(s.nt > 0 && s.nphi > 0 && s.n_blocks % 2 == 1 && s.n_blocks >= 1, "angular grid sizes invalid");
+  require(s.nphi >= 2 * s.mj_max + 1, "n_phi < 2*MjMax + 1");
+  require(s.i0 >= 0 && s.i0 < s.n_rot, "initial_channel out of range");
+  require(s.spa >= 1, "steps_per_analysis must be >= 1");
+  require(s.n_rep >= 1 && s.n_rep <= s.n_xy() && s.n_ops >= 1, "symmetry sizes invalid");
+  require(s.ra >= 0 && s.rb < s.nr, "r absorber range invalid");
+  require(d.precision == SPO_PRECISION_FP64 || d.precision == SPO_PRECISION_MIXED, "unknown precision");
+  return s;
+}
+
+}  // namespace
+
+struct spo_handle {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Sizes s{};
+  std::unique_ptr<StepBase> impl;
+};
+
+namespace {
+template <typename F>
+int guarded(spo_handle* h, F&& f) {
+  if (!h) return SPO_ERR_INVALID;
+  try {
+    check_cuda(cudaSetDevice(h->device), "cudaSetDevice");
+    f();
+    return SPO_OK;
+  } catch (const SpoError& e) {
+    h->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    h->err = e.what();
+    return SPO_ERR_DEVICE;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+const char* spo_version(void) { return SPO_B200_VERSION; }
+
+const char* spo_last_error(const spo_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int spo_create(const spo_desc* desc, spo_handle** out) {
+  if (!out) return SPO_ERR_INVALID;
+  *out = nullptr;
+  auto h = std::make_unique<spo_handle>();
+  try {
+    require(desc != nullptr, "descriptor is null");
+    h->s = sizes_of(*desc);
+    h->device = desc->device;
+    check_cuda(cudaSetDevice(h->device), "cudaSetDevice");
+    check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (desc->precision == SPO_PRECISION_FP64)
+      h->impl = std::make_unique<Step<double>>(*desc, h->s, h->stream);
+    else
+      h->impl = std::make_unique<Step<float>>(*desc, h->s, h->stream);
+  } catch (const SpoError& e) {
+    g_create_error = e.what();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    return SPO_ERR_DEVICE;
+  }
+  *out = h.release();
+  return SPO_OK;
+}
+
+int spo_destroy(spo_handle* h) {
+  if (!h) return SPO_OK;
+  cudaSetDevice(h->device);
+  h->impl.reset();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return SPO_OK;
+}
+
+int spo_propagate_analysis_step(spo_handle* h) {
+  return guarded(h, [&] { h->impl->propagate_analysis_step(); });
+}
+
+int spo_upload_state(spo_handle* h, const double* psi, const double* chi) {
+  return guarded(h, [&] { h->impl->upload(psi, chi); });
+}
+
+int spo_download_state(spo_handle* h, double* psi, double* chi) {
+  return guarded(h, [&] { h->impl->download(psi, chi); });
+}
+
+int spo_get_specular(spo_handle* h, double* chi) {
+  return guarded(h, [&] {
+    require(chi != nullptr, "chi is null");
+    h->impl->download(nullptr, chi);
+  });
+}
+
+int spo_get_z_plane(spo_handle* h, int iz, double* out) {
+  return guarded(h, [&] {
+    require(out != nullptr, "out is null");
+    h->impl->z_plane(iz, out);
+  });
+}
+
+int spo_block_densities(spo_handle* h, double* out) {
+  return guarded(h, [&] {
+    require(out != nullptr, "out is null");
+    h->impl->block_densities(out);
+  });
+}
+
+int spo_site_column(spo_handle* h, int ixy, double* out) {
+  return guarded(h, [&] {
+    require(out != nullptr, "out is null");
+    h->impl->site_column(ixy, out);
+  });
+}
+
+int spo_apply_stage(spo_handle* h, int stage, int half_step) {
+  return guarded(h, [&] { h->impl->apply_stage(stage, half_step != 0); });
+}
+
+int spo_device_bytes(const spo_handle* h, unsigned long long* bytes) {
+  if (!h || !bytes) return SPO_ERR_INVALID;
+  *bytes = h->impl->bytes();
+  return SPO_OK;
+}
+
+int spo_last_launch_count(const spo_handle* h, int* launches) {
+  if (!h || !launches) return SPO_ERR_INVALID;
+  *launches = h->impl->launches();
+  return SPO_OK;
+}
+
+}  // extern "C"

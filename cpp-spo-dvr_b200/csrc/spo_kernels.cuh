@@ -1,0 +1,533 @@
+// Device code of the split-operator step: complex helpers, a shared-memory mixed-radix Stockham FFT,
+// and the kernels of one sub-step. Templated on the real type T (double: FP64 form, float: mixed form).
+//
+// Device layout of psi (the reference's host layout, src/propagation/wave_function.hpp:14-39):
+//   psi[irot + n_rot * (ixy + n_xy * izr)], ixy = iy + ny*ix, izr = ir + nr*iz.
+// Every FFT pass therefore moves tiles whose innermost (contiguous) index is a batch index, so the
+// global loads and stores of every kernel are coalesced, whatever axis is transformed.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace spo {
+
+// ---------------------------------------------------------------------------------------------
+// Complex arithmetic on double2 / float2
+// ---------------------------------------------------------------------------------------------
+template <typename T> struct VecOf;
+template <> struct VecOf<double> { using type = double2; };
+template <> struct VecOf<float> { using type = float2; };
+template <typename T> using Vec = typename VecOf<T>::type;
+
+template <typename V> __device__ __forceinline__ V cmake(decltype(V::x) re, decltype(V::x) im) {
+  V v;
+  v.x = re;
+  v.y = im;
+  return v;
+}
+template <typename V> __device__ __forceinline__ V cadd(V a, V b) { return cmake<V>(a.x + b.x, a.y + b.y); }
+template <typename V> __device__ __forceinline__ V csub(V a, V b) { return cmake<V>(a.x - b.x, a.y - b.y); }
+template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
+  return cmake<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename V> __device__ __forceinline__ V cconj(V a) { return cmake<V>(a.x, -a.y); }
+template <typename V> __device__ __forceinline__ V cscale(V a, decltype(V::x) s) { return cmake<V>(a.x * s, a.y * s); }
+// i * s * a for s = +1 or -1.
+template <typename V> __device__ __forceinline__ V cimul(V a, int s) {
+  return s > 0 ? cmake<V>(-a.y, a.x) : cmake<V>(a.y, -a.x);
+}
+
+// ---------------------------------------------------------------------------------------------
+// FFT plan: the radices of one length, passed by value. Lengths are 2^h 3^i 5^j 7^k 11^m
+// (i <= 2, j, k, m <= 1), the reference's valid FFT sizes (src/fft/fft_sizes.cpp:9-34).
+// ---------------------------------------------------------------------------------------------
+constexpr int kMaxStages = 20;
+struct FftPlan {
+  int n;
+  int n_stages;
+  int radix[kMaxStages];
+};
+
+// w^q for the r-th roots of unity, read from the length-n table tw[k] = exp(-2 pi i k / n).
+template <typename V>
+__device__ __forceinline__ V root_of(const V* tw, int n, int r, int q, int sign) {
+  V w = tw[(q % r) * (n / r)];
+  return sign > 0 ? cconj(w) : w;
+}
+
+// In-register DFT of R values with exponent sign `sign`.
+template <typename V, int R>
+__device__ __forceinline__ void small_dft(V (&v)[R], const V* tw, int n, int sign) {
+  if constexpr (R == 2) {
+    const V a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    const V s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+    const V s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+    const V jd = cimul(d13, sign);
+    v[0] = cadd(s02, s13);
+    v[1] = cadd(d02, jd);
+    v[2] = csub(s02, s13);
+    v[3] = csub(d02, jd);
+  } else {
+    // Odd prime R: pairs (t, R - t) share the real part of the root and have opposite imaginary parts.
+    constexpr int H = R / 2;
+    V s[H + 1], d[H + 1];
+#pragma unroll
+    for (int t = 1; t <= H; ++t) {
+      s[t] = cadd(v[t], v[R - t]);
+      d[t] = csub(v[t], v[R - t]);
+    }
+    V out0 = v[0];
+#pragma unroll
+    for (int t = 1; t <= H; ++t) out0 = cadd(out0, s[t]);
+    V res[R];
+    res[0] = out0;
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      V re = v[0];
+      decltype(V::x) im_re = 0, im_im = 0;
+#pragma unroll
+      for (int t = 1; t <= H; ++t) {
+        const V w = root_of(tw, n, R, t * q, sign);
+        re = cadd(re, cscale(s[t], w.x));
+        im_re += w.y * d[t].x;
+        im_im += w.y * d[t].y;
+      }
+      const V rot = cmake<V>(-im_im, im_re);  // i * sum Im(w) d
+      res[q] = cadd(re, rot);
+      res[R - q] = csub(re, rot);
+    }
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = res[t];
+  }
+}
+
+// One Stockham stage of radix R for n_lines independent lines of length n stored in shared memory.
+// Line l starts at base(l) = (l / L1) * S1 + (l % L1), element e of a line is at base + e * S.
+// Consecutive threads take consecutive lines (conflict-free when lines are adjacent words).
+template <typename V, int R>
+__device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restrict__ dst, const V* tw, int n, int ns,
+                                          int sign, int n_lines, int L1, int S1, int S) {
+  const int m = n / R;
+  const int span = ns * R;
+  const int twstep = n / span;
+  const int total = n_lines * m;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int line = idx % n_lines;
+    const int j = idx / n_lines;
+    const int base = (line / L1) * S1 + (line % L1);
+    const int k = j % ns;
+    V v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = src[base + (j + t * m) * S];
+#pragma unroll
+    for (int t = 1; t < R; ++t) {
+      V w = tw[t * k * twstep];
+      if (sign > 0) w = cconj(w);
+      v[t] = cmul(v[t], w);
+    }
+    small_dft<V, R>(v, tw, n, sign);
+    const int o = (j / ns) * span + k;
+#pragma unroll
+    for (int t = 0; t < R; ++t) dst[base + (o + t * ns) * S] = v[t];
+  }
+}
+
+// Complete transform of the lines (see fft_stage), ping-ponging between a and b. Returns the buffer
+// that holds the result. Every stage ends with __syncthreads(); the caller must have synchronised
+// before the call.
+template <typename V>
+__device__ V* smem_fft(V* a, V* b, const V* tw, const FftPlan& p, int sign, int n_lines, int L1, int S1, int S) {
+  int ns = 1;
+  for (int s = 0; s < p.n_stages; ++s) {
+    const int r = p.radix[s];
+    switch (r) {
+      case 2: fft_stage<V, 2>(a, b, tw, p.n, ns, sign, n_lines, L1, S1, S); break;
+      case 3: fft_stage<V, 3>(a, b, tw, p.n, ns, sign, n_lines, L1, S1, S); break;
+      case 4: fft_stage<V, 4>(a, b, tw, p.n, ns, sign, n_lines, L1, S1, S); break;
+      case 5: fft_stage<V, 5>(a, b, tw, p.n, ns, sign, n_lines, L1, S1, S); break;
+      case 7: fft_stage<V, 7>(a, b, tw, p.n, ns, sign, n_lines, L1, S1, S); break;
+      case 11: fft_stage<V, 11>(a, b, tw, p.n, ns, sign, n_lines, L1, S1, S); break;
+      default: break;  // rejected at plan time
+    }
+    __syncthreads();
+    V* t = a;
+    a = b;
+    b = t;
+    ns *= r;
+  }
+  return a;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Axis pass: FFT along one axis of an array (outer, n, inner) with inner contiguous, for a tile of
+// `tb` consecutive inner elements: forward (sign -1), multiply by a factor, inverse (sign +1).
+// Used for T_Z and T_r of psi (src/propagation/kinetic_operators.cpp:77-111, separably) and for the
+// specular grid (src/propagation/specular_operator.cpp:48-54).
+// ---------------------------------------------------------------------------------------------
+enum AxisDir : int { kFwdFactorInv = 0, kFwdFactor = 1, kFactorInv = 2 };
+enum FactorMode : int { kNoFactor = 0, kFactorAxis = 1, kFactorAxisInner = 2 };
+
+template <typename T>
+struct AxisArgs {
+  Vec<T>* data;
+  long long inner;
+  FftPlan plan;
+  const Vec<T>* tw;      // exp(-2 pi i k / n), n values
+  const Vec<T>* factor;  // by axis index (kFactorAxis) or by inner + inner_count * k (kFactorAxisInner)
+  int factor_mode;
+  int dir;
+  const Vec<T>* post;    // pointwise factor by global element index after the pass, or null
+  int tb;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a) {
+  using V = Vec<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* buf0 = reinterpret_cast<V*>(smem_raw);
+  const int n = a.plan.n;
+  const int tb = a.tb;
+  V* buf1 = buf0 + n * tb;
+  V* tw = buf1 + n * tb;
+  const long long outer = blockIdx.y;
+  const long long i0 = static_cast<long long>(blockIdx.x) * tb;
+  const long long base = outer * n * a.inner + i0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) tw[k] = a.tw[k];
+  for (int e = threadIdx.x; e < n * tb; e += blockDim.x) {
+    const int k = e / tb, b = e % tb;
+    V v = cmake<V>(0, 0);
+    if (i0 + b < a.inner) v = a.data[base + k * a.inner + b];
+    buf0[e] = v;
+  }
+  __syncthreads();
+  V* cur = buf0;
+  V* oth = buf1;
+  if (a.dir != kFactorInv) {
+    cur = smem_fft(cur, oth, tw, a.plan, -1, tb, tb, 0, tb);
+    oth = cur == buf0 ? buf1 : buf0;
+  }
+  if (a.factor_mode != kNoFactor) {
+    for (int e = threadIdx.x; e < n * tb; e += blockDim.x) {
+      const int k = e / tb, b = e % tb;
+      const V f = a.factor_mode == kFactorAxis ? a.factor[k] : a.factor[(i0 + b) + a.inner * k];
+      cur[e] = cmul(f, cur[e]);
+    }
+    __syncthreads();
+  }
+  if (a.dir != kFwdFactor) {
+    cur = smem_fft(cur, oth, tw, a.plan, +1, tb, tb, 0, tb);
+  }
+  for (int e = threadIdx.x; e < n * tb; e += blockDim.x) {
+    const int k = e / tb, b = e % tb;
+    if (i0 + b < a.inner) {
+      const long long g = base + k * a.inner + b;
+      V v = cur[e];
+      if (a.post) v = cmul(a.post[g], v);
+      a.data[g] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// xy pass: exp(-i T_xy dt) at every (Z, r) point for a tile of `tb` rotational states: momentum
+// shift, 2D (x, y) FFT, kinetic factor, inverse, shift back (src/propagation/kinetic_operators.cpp:
+// 134-172). In the gas-phase region (izr >= izr_gas_first) the potential step of that region,
+// optical_z * rot exp(-i vasy dt) rot (src/propagation/potential_operator.cpp:104-112), is applied
+// in the same pass when `apply_gas` is set.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+struct XyArgs {
+  Vec<T>* psi;
+  int n_rot, nx, ny;
+  FftPlan px, py;
+  const Vec<T>* twx;
+  const Vec<T>* twy;
+  const Vec<T>* factor;   // nx*ny, FFT scales folded in
+  const Vec<T>* shift_f;  // nx*ny or null (no momentum shift)
+  const Vec<T>* shift_b;
+  int tb;
+  int apply_gas;
+  long long izr_gas_first;
+  int nr;
+  const T* opt_z;          // nz
+  const Vec<T>* gas_step;  // (ir, irot): opt_r rot gas rot
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) xy_pass_kernel(XyArgs<T> a) {
+  using V = Vec<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nxy = a.nx * a.ny;
+  const int tb = a.tb;
+  V* buf0 = reinterpret_cast<V*>(smem_raw);
+  V* buf1 = buf0 + nxy * tb;
+  V* twx = buf1 + nxy * tb;
+  V* twy = twx + a.nx;
+  const long long izr = blockIdx.y;
+  const int r0 = blockIdx.x * tb;
+  for (int k = threadIdx.x; k < a.nx; k += blockDim.x) twx[k] = a.twx[k];
+  for (int k = threadIdx.x; k < a.ny; k += blockDim.x) twy[k] = a.twy[k];
+  const long long col0 = izr * nxy;
+  for (int e = threadIdx.x; e < nxy * tb; e += blockDim.x) {
+    const int ixy = e / tb, b = e % tb;
+    V v = cmake<V>(0, 0);
+    if (r0 + b < a.n_rot) {
+      v = a.psi[(col0 + ixy) * a.n_rot + r0 + b];
+      if (a.shift_f) v = cmul(v, a.shift_f[ixy]);
+    }
+    buf0[e] = v;
+  }
+  __syncthreads();
+  // y: lines (ix, b), element stride tb; x: lines (iy, b), element stride ny*tb.
+  V* cur = smem_fft(buf0, buf1, twy, a.py, -1, a.nx * tb, tb, a.ny * tb, tb);
+  V* oth = cur == buf0 ? buf1 : buf0;
+  cur = smem_fft(cur, oth, twx, a.px, -1, a.ny * tb, a.ny * tb, 0, a.ny * tb);
+  oth = cur == buf0 ? buf1 : buf0;
+  for (int e = threadIdx.x; e < nxy * tb; e += blockDim.x) cur[e] = cmul(a.factor[e / tb], cur[e]);
+  __syncthreads();
+  cur = smem_fft(cur, oth, twx, a.px, +1, a.ny * tb, a.ny * tb, 0, a.ny * tb);
+  oth = cur == buf0 ? buf1 : buf0;
+  cur = smem_fft(cur, oth, twy, a.py, +1, a.nx * tb, tb, a.ny * tb, tb);
+  const bool gas = a.apply_gas && izr >= a.izr_gas_first;
+  const int ir = static_cast<int>(izr % a.nr);
+  const T oz = gas ? a.opt_z[izr / a.nr] : T(1);
+  for (int e = threadIdx.x; e < nxy * tb; e += blockDim.x) {
+    const int ixy = e / tb, b = e % tb;
+    if (r0 + b < a.n_rot) {
+      V v = cur[e];
+      if (a.shift_b) v = cmul(v, a.shift_b[ixy]);
+      if (gas) {
+        v = cmul(a.gas_step[ir * a.n_rot + r0 + b], v);
+        v = cscale(v, oz);
+      }
+      a.psi[(col0 + ixy) * a.n_rot + r0 + b] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Potential step of the interaction region, one (Z, r) point per block, all its (x, y) columns
+// (src/propagation/potential_operator.cpp:114-136, 158-201; src/propagation/angular_transform.cpp:
+// 54-114): absorption and rot(dt/2), the specular wave added to the initial channel, FBR -> DVR
+// (theta contraction per mJ block, phi FFT sign +1), exp(i A) through the symmetry maps, DVR -> FBR
+// (phi FFT sign -1, transposed contraction), rot(dt/2), and the projection of the initial channel
+// onto the specular grid with a fixed summation order.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+struct PotArgs {
+  Vec<T>* psi;
+  Vec<T>* chi;                // (ir, iz)
+  int n_rot, n_xy, nr, n_theta, n_phi, ld, n_blocks, mj_max, initial_channel, n_rep;
+  int cb;                     // columns per chunk
+  FftPlan pphi;
+  const Vec<T>* twphi;
+  const T* legendre;          // (block, theta, J)
+  const int* block_first;     // per mJ block: first irot
+  const int* block_size;      // n_J
+  const int* block_slot;      // phi slot
+  const int* block_offset;    // offset into legendre
+  const int* irot_block;      // block of each irot
+  const T* opt_z;             // nz
+  const Vec<T>* before;       // (ir, irot): opt_r rot(dt/2)
+  const Vec<T>* rot_half;     // (ir, irot)
+  const Vec<T>* sp2sc;        // n_xy
+  const Vec<T>* sc2sp;        // n_xy
+  const Vec<T>* expia;        // (izr, irep, theta, phi)
+  const int* rep_of;          // n_xy
+  const int* phi_map;         // n_xy * n_phi: phi_index of the operation of each ixy
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
+  using V = Vec<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n_rot = a.n_rot, nt = a.n_theta, nphi = a.n_phi, ld = a.ld, cb = a.cb;
+  const int dvr_col = nt * ld;
+  V* fbr = reinterpret_cast<V*>(smem_raw);   // cb * n_rot
+  V* dvr0 = fbr + cb * n_rot;                // cb * nt * ld
+  V* dvr1 = dvr0 + cb * dvr_col;             // cb * nt * ld
+  V* twp = dvr1 + cb * dvr_col;              // nphi
+  V* i0buf = twp + nphi;                     // n_xy
+  V* red = i0buf + a.n_xy;                   // 32
+  T* leg = reinterpret_cast<T*>(red + 32);   // nt * n_rot
+  const int izr = blockIdx.x;
+  const int ir = izr % a.nr;
+  const int iz = izr / a.nr;
+  const int i0 = a.initial_channel;
+  for (int k = threadIdx.x; k < nphi; k += blockDim.x) twp[k] = a.twphi[k];
+  for (int k = threadIdx.x; k < nt * n_rot; k += blockDim.x) leg[k] = a.legendre[k];
+  const T oz = a.opt_z[iz];
+  const V incoming = a.chi[ir + a.nr * iz];
+  const V rot_i0 = a.rot_half[ir * n_rot + i0];
+  const long long col_base = static_cast<long long>(izr) * a.n_xy;
+  const long long e_base = static_cast<long long>(izr) * a.n_rep * nt * nphi;
+  __syncthreads();
+
+  for (int c0 = 0; c0 < a.n_xy; c0 += cb) {
+    const int ncol = min(cb, a.n_xy - c0);
+    // Load, absorb, rot(dt/2), add the specular wave to the initial channel.
+    for (int e = threadIdx.x; e < ncol * n_rot; e += blockDim.x) {
+      const int c = e / n_rot, irot = e % n_rot;
+      const int ixy = c0 + c;
+      V v = a.psi[(col_base + ixy) * n_rot + irot];
+      v = cscale(cmul(a.before[ir * n_rot + irot], v), oz);
+      if (irot == i0) v = cadd(v, cmul(rot_i0, cmul(a.sp2sc[ixy], incoming)));
+      fbr[c * n_rot + irot] = v;
+    }
+    __syncthreads();
+    // FBR -> DVR: theta sums per mJ block into the block's phi slot; other slots zero.
+    for (int e = threadIdx.x; e < ncol * nt * nphi; e += blockDim.x) {
+      const int p = e % nphi;
+      const int t = (e / nphi) % nt;
+      const int c = e / (nphi * nt);
+      // slot p holds mJ = p (p <= mj_max) or mJ = p - nphi (p >= nphi - mj_max)
+      int blk = -1;
+      if (p <= a.mj_max) blk = a.mj_max + p;
+      else if (p >= nphi - a.mj_max) blk = a.mj_max + (p - nphi);
+      V s = cmake<V>(0, 0);
+      if (blk >= 0) {
+        const int nj = a.block_size[blk];
+        const T* row = leg + a.block_offset[blk] + t * nj;
+        const V* f = fbr + c * n_rot + a.block_first[blk];
+        for (int j = 0; j < nj; ++j) s = cadd(s, cscale(f[j], row[j]));
+      }
+      dvr0[c * dvr_col + t * ld + p] = s;
+    }
+    __syncthreads();
+    V* cur = smem_fft(dvr0, dvr1, twp, a.pphi, +1, ncol * nt, 1, ld, 1);
+    V* oth = cur == dvr0 ? dvr1 : dvr0;
+    // exp(i A) of the representative, at the mapped phi.
+    for (int e = threadIdx.x; e < ncol * nt * nphi; e += blockDim.x) {
+      const int p = e % nphi;
+      const int t = (e / nphi) % nt;
+      const int c = e / (nphi * nt);
+      const int ixy = c0 + c;
+      const int rep = a.rep_of[ixy];
+      const int pm = a.phi_map[ixy * nphi + p];
+      const V b = a.expia[e_base + (static_cast<long long>(rep) * nt + t) * nphi + pm];
+      cur[c * dvr_col + t * ld + p] = cmul(b, cur[c * dvr_col + t * ld + p]);
+    }
+    __syncthreads();
+    cur = smem_fft(cur, oth, twp, a.pphi, -1, ncol * nt, 1, ld, 1);
+    // DVR -> FBR: transposed theta sums, then rot(dt/2).
+    for (int e = threadIdx.x; e < ncol * n_rot; e += blockDim.x) {
+      const int c = e / n_rot, irot = e % n_rot;
+      const int blk = a.irot_block[irot];
+      const int nj = a.block_size[blk];
+      const int jj = irot - a.block_first[blk];
+      const int slot = a.block_slot[blk];
+      const T* col = leg + a.block_offset[blk] + jj;
+      V s = cmake<V>(0, 0);
+      for (int t = 0; t < nt; ++t) s = cadd(s, cscale(cur[c * dvr_col + t * ld + slot], col[t * nj]));
+      s = cmul(a.rot_half[ir * n_rot + irot], s);
+      const int ixy = c0 + c;
+      if (irot == i0) i0buf[ixy] = s;
+      else a.psi[(col_base + ixy) * n_rot + irot] = s;
+    }
+    __syncthreads();
+  }
+  // Projection onto the specular grid: a fixed-order sum over (x, y) by warp 0.
+  if (threadIdx.x < 32) {
+    V s = cmake<V>(0, 0);
+    for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += 32) s = cadd(s, cmul(a.sc2sp[ixy], i0buf[ixy]));
+    red[threadIdx.x] = s;
+    __syncwarp();
+    if (threadIdx.x == 0) {
+      V p = cmake<V>(0, 0);
+      for (int k = 0; k < 32; ++k) p = cadd(p, red[k]);
+      red[0] = p;
+      a.chi[ir + a.nr * iz] = p;
+    }
+  }
+  __syncthreads();
+  const V proj = red[0];
+  for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += blockDim.x)
+    a.psi[(col_base + ixy) * n_rot + i0] = csub(i0buf[ixy], cmul(a.sp2sc[ixy], proj));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Utilities
+// ---------------------------------------------------------------------------------------------
+
+// Potential step of the gas-phase region alone (izr >= izr_first): optical_z * gas_step(ir, irot)
+// (src/propagation/potential_operator.cpp:104-112). The propagation fuses this into the xy pass;
+// this kernel serves the stage-by-stage entry point.
+template <typename T>
+__global__ void gas_phase_kernel(Vec<T>* __restrict__ psi, long long izr_first, long long n_zr, int n_rot, int n_xy,
+                                 int nr, const T* __restrict__ opt_z, const Vec<T>* __restrict__ gas_step) {
+  const long long per_izr = static_cast<long long>(n_xy) * n_rot;
+  const long long n = (n_zr - izr_first) * per_izr;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long izr = izr_first + i / per_izr;
+    const int irot = static_cast<int>(i % n_rot);
+    const int ir = static_cast<int>(izr % nr);
+    const long long g = izr_first * per_izr + i;
+    psi[g] = cscale(cmul(gas_step[ir * n_rot + irot], psi[g]), opt_z[izr / nr]);
+  }
+}
+
+// exp(i A), A = -V dt, formed in FP64 (src/propagation/potential_operator.cpp:55-65 with
+// src/potential/potential_grid.cpp:164-167), then rounded to T.
+template <typename T>
+__global__ void exp_potential_kernel(const double* __restrict__ v, Vec<T>* __restrict__ out, long long n, double dt) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const double a = -v[i] * dt;
+    double s, c;
+    sincos(a, &s, &c);
+    out[i] = cmake<Vec<T>>(static_cast<T>(c), static_cast<T>(s));
+  }
+}
+
+// sum |psi|^2 over one (Z, r) block (n_block values) in FP64, fixed order: strided per thread, then
+// a fixed tree (src/propagation/averages.cpp:20-29).
+template <typename T>
+__global__ void block_density_kernel(const Vec<T>* __restrict__ psi, long long n_block, double* __restrict__ out) {
+  __shared__ double part[256];
+  const long long base = static_cast<long long>(blockIdx.x) * n_block;
+  double s = 0.0;
+  for (long long i = threadIdx.x; i < n_block; i += blockDim.x) {
+    const Vec<T> v = psi[base + i];
+    const double re = v.x, im = v.y;
+    s += re * re + im * im;
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = part[0];
+}
+
+// (izr, irot) column of one (x, y) point: out[izr + n_zr * irot] = psi[irot + n_rot*(ixy + n_xy*izr)].
+template <typename T>
+__global__ void site_column_kernel(const Vec<T>* __restrict__ psi, double2* __restrict__ out, int n_rot, int n_xy,
+                                   long long n_zr, int ixy) {
+  const long long n = n_zr * n_rot;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long izr = i % n_zr;
+    const int irot = static_cast<int>(i / n_zr);
+    const Vec<T> v = psi[(izr * n_xy + ixy) * n_rot + irot];
+    out[i] = make_double2(v.x, v.y);
+  }
+}
+
+// Precision conversion of a complex array.
+template <typename TO, typename TI>
+__global__ void convert_kernel(const Vec<TI>* __restrict__ in, Vec<TO>* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const Vec<TI> v = in[i];
+    out[i] = cmake<Vec<TO>>(static_cast<TO>(v.x), static_cast<TO>(v.y));
+  }
+}
+
+}  // namespace spo

@@ -1,0 +1,161 @@
+"""B200Backend: the reference's PropagationBackend interface over the C ABI.
+
+Mirrors spodvr::PropagationBackend (src/propagation/propagation_backend.hpp:34-59) member by
+member, with the same layouts (src/propagation/wave_function.hpp) and the same meaning:
+
+  read_wave_packet(psi, chi) ...... PropagationBackend::read_wave_packet (restart)
+  wave_packet_on_host() ........... PropagationBackend::wave_packet_on_host (checkpoint, dump)
+  propagate_analysis_step() ....... PropagationBackend::propagate_analysis_step
+  specular() ...................... PropagationBackend::specular
+  z_plane(iz) ..................... PropagationBackend::z_plane
+  block_densities() ............... PropagationBackend::block_densities
+  site_column(ixy) ................ PropagationBackend::site_column
+
+Errors: the reference throws (InputError, CudaError); here a non-zero status raises B200Error
+carrying the library's message. Construction takes a CaseBundle, the file form of BackendInput +
+PotentialGrid + SpecularWave (propagation_backend.hpp:63-74).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .case import CaseBundle
+
+
+def _c(x):
+    return np.ascontiguousarray(x, dtype=np.complex128)
+
+
+def _f(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def _i(x):
+    return np.ascontiguousarray(x, dtype=np.int32)
+
+
+class B200Backend:
+    """One wave packet resident on a B200, propagated by the sm_100a kernels of libspo_b200."""
+
+    def __init__(self, case: CaseBundle, precision: str = "fp64", device: int = 0):
+        self.case = case
+        self._lib = capi.lib()
+        m = case.m
+        blocks = np.asarray(m["mj_blocks"], dtype=np.int32).reshape(-1, 3)
+        keep = {
+            "first": _i(blocks[:, 0]), "size": _i(blocks[:, 1]), "slot": _i(blocks[:, 2]),
+        }
+        for name in case.a:
+            arr = case.a[name]
+            keep[name] = _c(arr) if arr.dtype == np.complex128 else (_i(arr) if arr.dtype == np.int32 else _f(arr))
+        self._keep = keep  # alive while the descriptor is read
+        d = capi.SpoDesc()
+        for key in ["n_rot", "nx", "ny", "nr", "nz", "nz_potential", "nz_specular", "n_theta", "n_phi",
+                    "initial_channel", "r_absorber_first", "r_absorber_last", "steps_per_analysis", "n_rep",
+                    "n_ops"]:
+            setattr(d, key, int(m[key]))
+        d.time_step = float(m["time_step"])
+        for key in ["fft_scale_z", "fft_scale_r", "fft_scale_x", "fft_scale_y"]:
+            setattr(d, key, float(m[key]))
+        d.n_mj_blocks = int(blocks.shape[0])
+        d.mj_fbr_first = capi.iptr(keep["first"])
+        d.mj_fbr_size = capi.iptr(keep["size"])
+        d.mj_phi_slot = capi.iptr(keep["slot"])
+        for name in ["legendre", "z_kinetic_full", "z_kinetic_half", "r_kinetic_full", "r_kinetic_half",
+                     "xy_kinetic_full", "xy_kinetic_half", "specular_kinetic_full", "specular_kinetic_half",
+                     "rotation_half", "z_optical", "r_optical", "z_specular_optical", "gas_phase", "shift_forward",
+                     "shift_backward", "specular_to_scattering", "scattering_to_specular", "potential",
+                     "chi_initial"]:
+            setattr(d, name, capi.dptr(keep[name]))
+        for name in ["representative_of", "operation_of", "phi_index"]:
+            setattr(d, name, capi.iptr(keep[name]))
+        d.precision = capi.PRECISION_MIXED if precision == "mixed" else capi.PRECISION_FP64
+        d.device = int(device)
+        self.precision = precision
+        h = ctypes.c_void_p()
+        st = self._lib.spo_create(ctypes.byref(d), ctypes.byref(h))
+        self._keep = None
+        if st != capi.SPO_OK:
+            raise capi.B200Error(st, self._lib.spo_last_error(None).decode())
+        self._h = h
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.spo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int):
+        if status != capi.SPO_OK:
+            raise capi.B200Error(status, self._lib.spo_last_error(self._h).decode())
+
+    # ------------------------------------------------------------------ PropagationBackend
+    def read_wave_packet(self, psi: np.ndarray | None, chi: np.ndarray | None) -> None:
+        p = None if psi is None else _c(psi).reshape(-1)
+        c = None if chi is None else _c(chi).reshape(-1)
+        if p is not None and p.size != int(np.prod(self.case.psi_shape)):
+            raise ValueError("psi has the wrong size")
+        if c is not None and c.size != int(np.prod(self.case.chi_shape)):
+            raise ValueError("chi has the wrong size")
+        self._check(self._lib.spo_upload_state(self._h, capi.dptr(p), capi.dptr(c)))
+
+    def wave_packet_on_host(self):
+        psi = np.empty(self.case.psi_shape, dtype=np.complex128)
+        chi = np.empty(self.case.chi_shape, dtype=np.complex128)
+        self._check(self._lib.spo_download_state(self._h, capi.dptr(psi), capi.dptr(chi)))
+        return psi, chi
+
+    def propagate_analysis_step(self) -> None:
+        self._check(self._lib.spo_propagate_analysis_step(self._h))
+
+    def specular(self, out: np.ndarray | None = None) -> np.ndarray:
+        chi = np.empty(self.case.chi_shape, dtype=np.complex128) if out is None else out
+        self._check(self._lib.spo_get_specular(self._h, capi.dptr(chi)))
+        return chi
+
+    def z_plane(self, iz: int, out: np.ndarray | None = None) -> np.ndarray:
+        c = self.case
+        plane = np.empty((c.nr, c.nx, c.ny, c.n_rot), dtype=np.complex128) if out is None else out
+        self._check(self._lib.spo_get_z_plane(self._h, int(iz), capi.dptr(plane)))
+        return plane
+
+    def block_densities(self) -> np.ndarray:
+        out = np.empty(self.case.nz * self.case.nr, dtype=np.float64)
+        self._check(self._lib.spo_block_densities(self._h, capi.dptr(out)))
+        return out
+
+    def site_column(self, ixy: int) -> np.ndarray:
+        c = self.case
+        out = np.empty((c.n_rot, c.nz * c.nr), dtype=np.complex128)
+        self._check(self._lib.spo_site_column(self._h, int(ixy), capi.dptr(out)))
+        return out
+
+    # ------------------------------------------------------------------ diagnostics
+    def apply_stage(self, stage: int, half: bool = False) -> None:
+        self._check(self._lib.spo_apply_stage(self._h, int(stage), 1 if half else 0))
+
+    def device_bytes(self) -> int:
+        v = ctypes.c_ulonglong()
+        self._check(self._lib.spo_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    def last_launch_count(self) -> int:
+        v = ctypes.c_int()
+        self._check(self._lib.spo_last_launch_count(self._h, ctypes.byref(v)))
+        return v.value

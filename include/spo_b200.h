@@ -1,0 +1,169 @@
+/*
+ * spo_b200.h - C ABI of the B200 (sm_100a) split-operator propagation step.
+ *
+ * A drop-in for the propagation backend of SPO-DVR: every entry point below replaces one member of
+ * the reference's PropagationBackend interface (src/propagation/propagation_backend.hpp:34-59) or
+ * of its construction (BackendInput + BackendFactory, propagation_backend.hpp:63-74). The
+ * descriptor carries exactly the data a backend is built from there: the grid sizes, the
+ * precomputed FP64 factor tables (PropagationTables, src/propagation/propagation_tables.hpp:26-72),
+ * the angular transform tables (AngularTransform::mj_blocks/matrix, angular_transform.hpp:67-76),
+ * the surface-symmetry maps and the potential grid in hartree (PotentialGrid,
+ * src/potential/potential_grid.hpp:21-37) and the initial specular wave.
+ *
+ * Conventions:
+ *   - plain C types only; complex numbers are interleaved (re, im) pairs of double;
+ *   - every call returns an int status (SPO_OK = 0); no exception crosses the ABI;
+ *     spo_last_error(h) gives the message of the last failure of a handle;
+ *   - a handle owns all its device memory and one CUDA stream; it is not thread-safe;
+ *     every call is synchronous with respect to the host buffers it is given;
+ *   - the host-side layouts are the reference's host layouts (src/propagation/wave_function.hpp):
+ *       psi[irot + n_rot*(ixy + nx*ny*izr)], ixy = iy + ny*ix, izr = ir + nr*iz
+ *       chi[ir + nr*iz] on the specular Z grid.
+ *   - the device layout of psi is the same (irot fastest), so readbacks are plain copies.
+ */
+#ifndef SPO_B200_H
+#define SPO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPO_B200_VERSION "0.1.0"
+
+/* Status codes. */
+enum spo_status {
+  SPO_OK = 0,
+  SPO_ERR_INVALID = 1,   /* invalid argument or descriptor (reference: InputError / invalid_argument) */
+  SPO_ERR_OOM = 2,       /* device memory exhausted (reference: check_device_memory, NotSupportedError) */
+  SPO_ERR_DEVICE = 3,    /* CUDA error (reference: CudaError, src/cuda/cuda_error.hpp:10-23) */
+  SPO_ERR_TIMEOUT = 4,   /* a bounded device-side wait gave up */
+  SPO_ERR_STATE = 5      /* call not valid in the handle's current state */
+};
+
+/* Arithmetic of the step: FP64 (complex128 psi, FP64 FFTs and factors), or mixed (complex64 psi,
+ * FP32 FFTs and factors rounded once from the FP64 tables; exp(-iV dt) formed in FP64 on the
+ * device, then rounded). */
+enum spo_precision { SPO_PRECISION_FP64 = 0, SPO_PRECISION_MIXED = 1 };
+
+/* Everything a propagation backend is built from (BackendInput + PotentialGrid + SpecularWave).
+ * All pointers are host pointers, read during spo_create only. */
+typedef struct spo_desc {
+  /* --- grid sizes ------------------------------------------------------------------------ */
+  int n_rot;            /* rotational FBR basis size, RotationalBasis::size() */
+  int nx, ny, nr, nz;   /* scattering grid */
+  int nz_potential;     /* Z points with Z < zasymp (SpatialGrids::nz_potential) */
+  int nz_specular;      /* specular Z grid */
+  int n_theta, n_phi;   /* angular DVR grid */
+  int initial_channel;  /* RotationalBasis::initial_index() */
+  int r_absorber_first, r_absorber_last;  /* SpatialGrids::r_optical (inclusive) */
+  int steps_per_analysis;                 /* Config::derived.steps_per_analysis (nanspo) */
+  double time_step;                       /* dtStep (hartree^-1 units of the reference) */
+
+  /* --- angular transform (AngularTransform::mj_blocks / matrix) ---------------------------- */
+  int n_mj_blocks;             /* 2*MjMax + 1, in the order mJ = -MjMax .. MjMax */
+  const int* mj_fbr_first;     /* first FBR index of each block */
+  const int* mj_fbr_size;      /* number of J values of each block */
+  const int* mj_phi_slot;      /* phi FFT slot of each block's mJ */
+  const double* legendre;      /* sqrt(w_t/nphi) P_J^m(theta_t), ordered (block, theta, J) */
+
+  /* --- factor tables (PropagationTables), complex as (re, im) pairs ------------------------ */
+  const double* z_kinetic_full;        /* nz  */
+  const double* z_kinetic_half;        /* nz  (principal square root of the full step) */
+  const double* r_kinetic_full;        /* nr  */
+  const double* r_kinetic_half;        /* nr  */
+  const double* xy_kinetic_full;       /* nx*ny */
+  const double* xy_kinetic_half;       /* nx*ny */
+  const double* specular_kinetic_full; /* nr*nz_specular, (ir, iz) */
+  const double* specular_kinetic_half; /* nr*nz_specular */
+  const double* rotation_half;         /* n_rot*nr, (irot, ir): exp(-i E_rot dt/2) */
+  const double* z_optical;             /* nz, real: exp(-V_opt dt) */
+  const double* r_optical;             /* nr, real */
+  const double* z_specular_optical;    /* nz_specular, real */
+  const double* gas_phase;             /* nr: exp(-i vasy(r) dt) */
+  const double* shift_forward;         /* nx*ny: exp(-i k0.R) */
+  const double* shift_backward;        /* nx*ny */
+  const double* specular_to_scattering;  /* nx*ny */
+  const double* scattering_to_specular;  /* nx*ny */
+  double fft_scale_z, fft_scale_r, fft_scale_x, fft_scale_y;
+
+  /* --- potential on the interaction region (PotentialGrid) --------------------------------- */
+  int n_rep;                    /* (x, y) representatives of the surface symmetry */
+  int n_ops;                    /* usable symmetry operations */
+  const double* potential;      /* V (hartree), (itp, irep, izr), itp = iphi + nphi*itheta, izr < nz_potential*nr */
+  const int* representative_of; /* nx*ny */
+  const int* operation_of;      /* nx*ny */
+  const int* phi_index;         /* n_ops*n_phi */
+
+  /* --- initial state and options ----------------------------------------------------------- */
+  const double* chi_initial;    /* nr*nz_specular complex: the initial packet; psi starts at zero */
+  int precision;                /* enum spo_precision */
+  int device;                   /* CUDA device ordinal */
+} spo_desc;
+
+typedef struct spo_handle spo_handle;
+
+/* Library version string. */
+const char* spo_version(void);
+
+/* Message of the last failed call on h (or of the last failed spo_create when h is NULL). */
+const char* spo_last_error(const spo_handle* h);
+
+/* Builds a backend: uploads the tables, forms exp(-iV dt) on the device in FP64, zeroes psi and
+ * sets chi to desc->chi_initial. Replaces the CpuBackend/CudaBackend constructors
+ * (src/propagation/cpu_backend.cpp:24-44) behind BackendFactory (propagation_backend.hpp:73-74). */
+int spo_create(const spo_desc* desc, spo_handle** out);
+
+/* Frees the handle and all its device memory. */
+int spo_destroy(spo_handle* h);
+
+/* [T(dt/2) V(dt) T(dt/2)]^n over one analysis step, n = steps_per_analysis.
+ * Replaces PropagationBackend::propagate_analysis_step (propagation_backend.hpp:47). */
+int spo_propagate_analysis_step(spo_handle* h);
+
+/* Replaces the wave packet (restart): psi (n_rot*nx*ny*nr*nz complex) and chi (nr*nz_specular
+ * complex) in host layout. Replaces PropagationBackend::read_wave_packet (propagation_backend.hpp:40). */
+int spo_upload_state(spo_handle* h, const double* psi, const double* chi);
+
+/* Copies the wave packet to the host layout (checkpoint). Either pointer may be NULL.
+ * Replaces PropagationBackend::wave_packet_on_host (propagation_backend.hpp:44). */
+int spo_download_state(spo_handle* h, double* psi, double* chi);
+
+/* The specular wave chi (nr*nz_specular complex). Replaces PropagationBackend::specular (:50). */
+int spo_get_specular(spo_handle* h, double* chi);
+
+/* The nr (Z, r) blocks of Z index iz, layout (irot, ixy, ir): n_rot*nx*ny*nr complex.
+ * Replaces PropagationBackend::z_plane (propagation_backend.hpp:52). */
+int spo_get_z_plane(spo_handle* h, int iz, double* out);
+
+/* sum |psi|^2 over (irot, ixy) at every izr (nz*nr doubles), summed in a fixed order on the
+ * device in FP64. Replaces PropagationBackend::block_densities (propagation_backend.hpp:55). */
+int spo_block_densities(spo_handle* h, double* out);
+
+/* The scattering wave at one (x, y) point, layout (izr, irot) with izr fastest (nz*nr*n_rot
+ * complex). Replaces PropagationBackend::site_column (propagation_backend.hpp:58). */
+int spo_site_column(spo_handle* h, int ixy, double* out);
+
+/* Operators of one sub-step, for stage-by-stage checks (the reference tests its operators one by one:
+ * tests/test_propagation.cpp, test_cuda_backend.cpp:161-278). */
+enum spo_stage {
+  SPO_STAGE_SPECULAR = 0,          /* SpecularOperator::apply, kinetic + gas phase + absorbers (specular_operator.cpp:40-45) */
+  SPO_STAGE_SPECULAR_KINETIC = 1,  /* SpecularOperator::apply with kinetic_only (the last half step) */
+  SPO_STAGE_ZR = 2,                /* ScatteringKineticOperator::apply_zr (kinetic_operators.cpp:77-111) */
+  SPO_STAGE_XY = 3,                /* ScatteringKineticOperator::apply_xy (kinetic_operators.cpp:114-124) */
+  SPO_STAGE_POTENTIAL = 4          /* PotentialOperator::apply (potential_operator.cpp:84-94) */
+};
+
+/* Applies one operator to the resident state, with the full (half_step = 0) or half (1) step's factors. */
+int spo_apply_stage(spo_handle* h, int stage, int half_step);
+
+/* Bytes of device memory the handle holds. */
+int spo_device_bytes(const spo_handle* h, unsigned long long* bytes);
+
+/* Number of kernel launches the last spo_propagate_analysis_step issued. */
+int spo_last_launch_count(const spo_handle* h, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPO_B200_H */
