@@ -1,0 +1,317 @@
+#!/usr/bin/env python
+"""Benchmark of the split-operator propagation step on B200: 6D grid-point-steps/s, mixed vs FP64.
+
+Workload: config 3 = the config-2 grid (nZ 128, nR 48, nX = nY 16, ntheta 16, nphi 32, n_rot 256,
+nZSpecular 512, dt 2, 5 time steps per analysis step; 8.05e8 6D points) in the mixed form, with the
+same workload in the FP64 form beside it. Seeded synthetic tables with the configuration's shapes
+(spo_b200.workload); the step does the same work whatever the values.
+
+One bench step = one analysis step (PropagationBackend::propagate_analysis_step: 5 time steps, i.e.
+6 kinetic sub-steps and 5 potential steps). value = 6D points * time steps / device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the reference's own CPU implementation of the step (oracle/_ref, the
+reference compiled from its sources) on the host cores, on a bounded sample of the same workload.
+Multi-GPU runs (torchrun) are independent replicas (one wave packet per GPU, as the reference's
+ensembles are run): no data-path collective, a barrier and a max-over-ranks of the device time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cpp-spo-dvr_b200"))
+
+METRIC = "6D SPO grid-point-steps/s on 1 B200, mixed vs FP64 at |ΔP_react|≤1e-6"
+UNIT = "grid-point-steps/s"
+CONFIG2_INPUT = os.path.join(ROOT, "tests", "golden", "inputs", "config2_dz.json")
+REF_TOOL = os.path.join(ROOT, "oracle", "_ref", "spo_ref_tool")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(", ") for r in open(self.path).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            for name, val in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], r[5:9]):
+                if val.strip() == "Active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def step_bytes(case, s: int) -> float:
+    """Algorithmic bytes of one time step: s (4 N_fbr + N_tab + 4 N_spec), N_fbr = nZ nR nX nY n_rot,
+    N_tab = nzpot nR n_rep ntheta nphi, N_spec = nZsp nR (psi read and written once for T and once for
+    V, the exp(-iV dt) table read once, chi likewise)."""
+    n_fbr = case.nz * case.nr * case.nx * case.ny * case.n_rot
+    n_tab = case.nz_potential * case.nr * case.n_rep * case.n_theta * case.n_phi
+    n_spec = case.nz_specular * case.nr
+    return s * (4.0 * n_fbr + n_tab + 4.0 * n_spec)
+
+
+def measure(case, precision, steps, warmup, device, world):
+    import numpy as np
+    import torch
+
+    from spo_b200 import B200Backend
+
+    be = B200Backend(case, precision=precision, device=device)
+    stream = torch.cuda.Stream(device=device)
+    be.set_stream(stream.cuda_stream)
+    # The initial wave packet: an empty scattering grid and the incoming packet on the specular grid.
+    psi0 = torch.zeros(case.psi_shape + (2,), dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)[..., 0]
+    chi0 = np.ascontiguousarray(case.a["chi_initial"].reshape(case.chi_shape))
+    be.read_wave_packet(psi0, chi0)
+    for _ in range(warmup):
+        be.propagate_analysis_step()
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(device)
+
+    # Device throughput: K analysis steps with the state resident in HBM.
+    barrier()
+    clocks = ClockSampler(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        be.propagate_analysis_step()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    clock = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = be.last_launch_count() * steps
+    barrier()
+
+    # Per-kernel CUDA-event times over the same K steps (a second pass, events around every launch).
+    be.profile(True)
+    for _ in range(steps):
+        be.propagate_analysis_step()
+    records = be.profile_records()
+    be.profile(False)
+    barrier()
+
+    # End to end through the C ABI with host buffers: the state uploaded from pinned host memory, then
+    # per analysis step the readbacks the reference's time loop makes (specular wave and the BK plane,
+    # src/propagation/propagation.cpp:81-84).
+    chi = torch.empty(case.chi_shape + (2,), dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)[..., 0]
+    plane = torch.empty((case.nr, case.nx, case.ny, case.n_rot, 2), dtype=torch.float64,
+                        pin_memory=True).numpy().view(np.complex128)[..., 0]
+    iz_a = int(case.m.get("iz_analysis", case.nz // 2))
+    e0.record(stream)
+    be.read_wave_packet(psi0, chi0)
+    for _ in range(steps):
+        be.propagate_analysis_step()
+        be.specular(out=chi)
+        be.z_plane(iz_a, out=plane)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    e2e_ms = e0.elapsed_time(e1)
+    h2d = (psi0.nbytes + chi0.nbytes) / steps
+    d2h = chi.nbytes + plane.nbytes
+    be.close()
+    return {"ms": ms, "launches": launches, "records": records, "clocks": clock, "e2e_ms": e2e_ms,
+            "h2d": h2d, "d2h": d2h}
+
+
+def reduce_max(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample_input(nx: int):
+    """The config-2 reference input with nX = nY = nx (a bounded sample for the CPU timings)."""
+    cfg = json.load(open(CONFIG2_INPUT))
+    cfg.update({"nX": nx, "nY": nx, "Title": f"config 2 sample, nX = nY = {nx}"})
+    path = tempfile.mktemp(suffix=".json")
+    json.dump(cfg, open(path, "w"))
+    return path
+
+
+def reference_timing(analysis_steps: int, warmup: int, nx: int = 4):
+    """The reference CPU path (oracle/_ref) on all host threads: JSON of spo_ref_tool time."""
+    if not os.path.exists(REF_TOOL):
+        return None, f"{REF_TOOL} is not built"
+    path = cpu_sample_input(nx)
+    env = dict(os.environ)
+    env.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    try:
+        r = subprocess.run([REF_TOOL, "time", path, "--analysis-steps", str(analysis_steps), "--warmup", str(warmup)],
+                           capture_output=True, text=True, env=env, timeout=1800)
+    finally:
+        os.unlink(path)
+    if r.returncode != 0:
+        return None, r.stderr.strip()[-300:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    out["sample"] = (f"config-2 reference input (Dai-Light PES, HD, JMax = MJMax = 15) with nX = nY = {nx}: "
+                     f"{int(out['n_points'])} 6D points, {analysis_steps} analysis steps of 5 time steps after "
+                     f"{warmup} warm-up; reference CpuBackend compiled from its sources (FFT: the project's FP64 "
+                     f"substitute, FFTW being absent)")
+    return out, None
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    out, err = reference_timing(args.steps, args.warmup)
+    if out is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    v = out["grid_point_steps_per_s"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * out["seconds"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "the reference's own set-up of the config-2 input (Dai-Light PES), bounded sample",
+            "config": {"workload": out["sample"], "step": "one analysis step = 5 time steps"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": out["threads"], "kind": "reference",
+                             "sample": out["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="config3", choices=["config3", "small"],
+                    help="small: the config-2 tables on nX = nY = 8 (psi 0.8 GB mixed, above L2), for profiler captures")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    from spo_b200 import workload
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device(f"cuda:{local}"))
+    case = workload.config_case({"nx": 8, "ny": 8} if args.workload == "small" else None)
+    res = {}
+    for precision in ("mixed", "fp64"):
+        res[precision] = measure(case, precision, args.steps, args.warmup, local, world)
+    time_steps = args.steps * case.steps_per_analysis
+    points = float(case.n_points)
+    out = {}
+    for precision, r in res.items():
+        ms = reduce_max(r["ms"], world, local)
+        e2e_ms = reduce_max(r["e2e_ms"], world, local)
+        out[precision] = {"ms": ms, "value": world * points * time_steps / (ms / 1000.0),
+                          "e2e": world * points * time_steps / (e2e_ms / 1000.0)}
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        m = res["mixed"]
+        top = max(m["records"], key=lambda r: r["ms"])
+        avg_ms = top["ms"] / top["launches"]
+        achieved = top["bytes_per_launch"] / (avg_ms / 1000.0) / 1e9
+        b_step = step_bytes(case, 8)
+        step_gbs = b_step * time_steps / (out["mixed"]["ms"] / 1000.0) / 1e9 / world
+        total_kernel_ms = sum(r["ms"] for r in m["records"])
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline and args.workload == "config3":
+            ref, err = reference_timing(1, 1)
+            if ref is not None:
+                cpu = {"value": ref["grid_point_steps_per_s"], "unit": UNIT, "cores": ref["threads"],
+                       "kind": "reference", "sample": ref["sample"]}
+            else:
+                cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": err}
+        line = {
+            "metric": METRIC, "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["mixed"]["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": ("config 3: config-2 grid nZ 128, nR 48, nX = nY 16, ntheta 16, nphi 32 "
+                                    "(JMax = MJMax = 15, n_rot 256), nZSpecular 512, nzpot 84, dt 2, mixed form "
+                                    "(complex64 psi, FP32 FFTs and factors, exp(-iV dt) formed in FP64)")
+                       if args.workload == "config3" else "small: config-2 tables on nX = nY = 8 (profiling)",
+                       "points": int(points), "step": "one analysis step = 5 time steps",
+                       "time_steps_per_step": case.steps_per_analysis,
+                       "l2": "inputs larger than L2 (psi 3.2 GB mixed / 6.4 GB FP64, table 2.6 / 5.3 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms"] / args.steps,
+                     "e2e": out["fp64"]["e2e"]},
+            "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+            "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "bytes_per_launch": top["bytes_per_launch"], "avg_launch_ms": avg_ms,
+                         "share_of_kernel_time": top["ms"] / total_kernel_ms},
+            "step_roofline": {"bytes_per_time_step": b_step, "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                              "frac": step_gbs / peak, "peak_kind": peak_kind},
+            "kernels": [{"name": r["name"], "launches": r["launches"], "ms": round(r["ms"], 4),
+                         "avg_ms": round(r["ms"] / r["launches"], 5),
+                         "gbs": round(r["bytes_per_launch"] / (r["ms"] / r["launches"] / 1000.0) / 1e9, 1)}
+                        for r in m["records"]],
+            "cpu_baseline": cpu,
+            "e2e": {"value": out["mixed"]["e2e"], "unit": UNIT, "h2d_bytes_per_step": int(m["h2d"]),
+                    "d2h_bytes_per_step": int(m["d2h"])},
+            "gpu_launches": m["launches"],
+            "clocks": m["clocks"],
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

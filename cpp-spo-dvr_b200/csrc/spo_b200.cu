@@ -129,6 +129,80 @@ struct Sizes {
   long long n_expia() const { return static_cast<long long>(nzp) * nr * n_rep * nt * nphi; }
 };
 
+// Per-kernel CUDA-event timing record.
+struct KernelRecord {
+  std::string name;
+  double ms = 0.0;
+  int launches = 0;
+  double bytes = 0.0;  // algorithmic bytes of one launch
+};
+
+// CUDA events around each launch, resolved after the stream is synchronised.
+class Profiler {
+ public:
+  ~Profiler() {
+    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+  }
+  void enable(bool on) {
+    on_ = on;
+    records_.clear();
+    pending_.clear();
+    used_ = 0;
+  }
+  bool on() const { return on_; }
+  // Returns the index of the pending pair; call end() after the launch.
+  void begin(cudaStream_t s) {
+    if (!on_) return;
+    check_cuda(cudaEventRecord(event(used_), s), "cudaEventRecord");
+  }
+  void end(cudaStream_t s, const char* name, double bytes) {
+    if (!on_) return;
+    check_cuda(cudaEventRecord(event(used_ + 1), s), "cudaEventRecord");
+    pending_.push_back({name, bytes, used_});
+    used_ += 2;
+  }
+  // After a synchronisation: adds the pending durations to the records.
+  void resolve() {
+    if (!on_) return;
+    for (const Pending& p : pending_) {
+      float ms = 0.0f;
+      check_cuda(cudaEventElapsedTime(&ms, pool_[p.first], pool_[p.first + 1]), "cudaEventElapsedTime");
+      KernelRecord* r = nullptr;
+      for (auto& x : records_)
+        if (x.name == p.name) r = &x;
+      if (!r) {
+        records_.push_back({p.name, 0.0, 0, p.bytes});
+        r = &records_.back();
+      }
+      r->ms += ms;
+      r->launches += 1;
+    }
+    pending_.clear();
+    used_ = 0;
+  }
+  const std::vector<KernelRecord>& records() const { return records_; }
+
+ private:
+  struct Pending {
+    std::string name;
+    double bytes;
+    std::size_t first;
+  };
+  cudaEvent_t event(std::size_t i) {
+    while (pool_.size() <= i) {
+      cudaEvent_t e;
+      check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+      pool_.push_back(e);
+    }
+    return pool_[i];
+  }
+  bool on_ = false;
+  std::vector<cudaEvent_t> pool_;
+  std::vector<Pending> pending_;
+  std::vector<KernelRecord> records_;
+  std::size_t used_ = 0;
+};
+
 class StepBase {
  public:
   virtual ~StepBase() = default;
@@ -141,6 +215,9 @@ class StepBase {
   virtual void apply_stage(int stage, bool half) = 0;
   virtual unsigned long long bytes() const = 0;
   virtual int launches() const = 0;
+  virtual void set_stream(cudaStream_t s) = 0;
+  virtual void profile(bool on) = 0;
+  virtual const std::vector<KernelRecord>& records() const = 0;
 };
 
 template <typename T>
@@ -148,7 +225,9 @@ class Step final : public StepBase {
   using V = spo::Vec<T>;
 
  public:
-  Step(const spo_desc& d, const Sizes& s, cudaStream_t stream) : s_(s), stream_(stream) { build(d); }
+  Step(const spo_desc& d, const Sizes& s, cudaStream_t stream) : s_(s), stream_(stream), own_stream_(stream) {
+    build(d);
+  }
 
   void propagate_analysis_step() override {
     launches_ = 0;
@@ -160,6 +239,7 @@ class Step final : public StepBase {
     }
     check_cuda(cudaGetLastError(), "propagate_analysis_step launch");
     check_cuda(cudaStreamSynchronize(stream_), "propagate_analysis_step");
+    prof_.resolve();
   }
 
   void upload(const double* psi, const double* chi) override {
@@ -217,10 +297,14 @@ class Step final : public StepBase {
     }
     check_cuda(cudaGetLastError(), "apply_stage launch");
     check_cuda(cudaStreamSynchronize(stream_), "apply_stage");
+    prof_.resolve();
   }
 
   unsigned long long bytes() const override { return arena_.bytes(); }
   int launches() const override { return launches_; }
+  void set_stream(cudaStream_t s) override { stream_ = s ? s : own_stream_; }
+  void profile(bool on) override { prof_.enable(on); }
+  const std::vector<KernelRecord>& records() const override { return prof_.records(); }
 
  private:
   // ------------------------------------------------------------------ one sub-step
@@ -233,17 +317,21 @@ class Step final : public StepBase {
 
   // Specular grid: r forward, Z forward * factor * inverse, r inverse (* W factors).
   void specular(bool half, bool kinetic_only) {
-    axis(chi_, /*outer*/ s_.nzs, plan_r_, tw_r_, /*inner*/ 1, nullptr, spo::kNoFactor, spo::kFwdFactor, nullptr);
-    axis(chi_, 1, plan_zs_, tw_zs_, s_.nr, half ? spec_half_ : spec_full_, spo::kFactorAxisInner,
+    const double b = 2.0 * sizeof(V) * s_.n_chi();
+    axis("specular_r", b, chi_, /*outer*/ s_.nzs, plan_r_, tw_r_, /*inner*/ 1, nullptr, spo::kNoFactor, spo::kFwdFactor,
+         nullptr);
+    axis("specular_z", b, chi_, 1, plan_zs_, tw_zs_, s_.nr, half ? spec_half_ : spec_full_, spo::kFactorAxisInner,
          spo::kFwdFactorInv, nullptr);
-    axis(chi_, s_.nzs, plan_r_, tw_r_, 1, nullptr, spo::kNoFactor, spo::kFactorInv, kinetic_only ? nullptr : spec_w_);
+    axis("specular_r", b, chi_, s_.nzs, plan_r_, tw_r_, 1, nullptr, spo::kNoFactor, spo::kFactorInv,
+         kinetic_only ? nullptr : spec_w_);
   }
 
   // T_Z and T_r of the scattering wave.
   void kinetic_zr(bool half) {
-    axis(psi_, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, spo::kFactorAxis,
+    const double b = 2.0 * sizeof(V) * s_.n_psi();
+    axis("kinetic_z", b, psi_, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, spo::kFactorAxis,
          spo::kFwdFactorInv, nullptr);
-    axis(psi_, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, spo::kFactorAxis,
+    axis("kinetic_r", b, psi_, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, spo::kFactorAxis,
          spo::kFwdFactorInv, nullptr);
   }
 
@@ -268,26 +356,33 @@ class Step final : public StepBase {
     x.opt_z = opt_z_;
     x.gas_step = gas_step_;
     const dim3 xg((s_.n_rot + xy_tb_ - 1) / xy_tb_, static_cast<unsigned>(s_.n_zr()));
+    prof_.begin(stream_);
     spo::xy_pass_kernel<T><<<xg, 256, xy_smem_, stream_>>>(x);
+    prof_.end(stream_, "kinetic_xy", 2.0 * sizeof(V) * s_.n_psi());
     ++launches_;
   }
 
   void gas_phase() {
     const long long first = static_cast<long long>(s_.nzp) * s_.nr;
     if (first >= s_.n_zr()) return;
+    prof_.begin(stream_);
     spo::gas_phase_kernel<T><<<1184, 256, 0, stream_>>>(psi_, first, s_.n_zr(), s_.n_rot, static_cast<int>(s_.n_xy()),
                                                         s_.nr, opt_z_, gas_step_);
+    prof_.end(stream_, "gas_phase", 2.0 * sizeof(V) * (s_.n_zr() - first) * s_.n_xy() * s_.n_rot);
     ++launches_;
   }
 
   void interaction() {
     if (s_.nzp == 0) return;
+    prof_.begin(stream_);
     spo::potential_kernel<T><<<static_cast<unsigned>(s_.nzp) * s_.nr, 256, pot_smem_, stream_>>>(pot_);
+    prof_.end(stream_, "potential",
+              sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia())));
     ++launches_;
   }
 
-  void axis(V* data, long long outer, const spo::FftPlan& plan, const V* tw, long long inner, const V* factor,
-            int factor_mode, int dir, const V* post) {
+  void axis(const char* name, double bytes, V* data, long long outer, const spo::FftPlan& plan, const V* tw,
+            long long inner, const V* factor, int factor_mode, int dir, const V* post) {
     spo::AxisArgs<T> a{};
     a.data = data;
     a.inner = inner;
@@ -300,7 +395,9 @@ class Step final : public StepBase {
     a.tb = axis_tile(plan.n, inner);
     const std::size_t smem = sizeof(V) * (2 * static_cast<std::size_t>(plan.n) * a.tb + plan.n);
     const dim3 grid(static_cast<unsigned>((inner + a.tb - 1) / a.tb), static_cast<unsigned>(outer));
+    prof_.begin(stream_);
     spo::axis_pass_kernel<T><<<grid, 256, smem, stream_>>>(a);
+    prof_.end(stream_, name, bytes);
     ++launches_;
   }
 
@@ -570,7 +667,9 @@ class Step final : public StepBase {
 
   Sizes s_;
   cudaStream_t stream_;
+  cudaStream_t own_stream_;
   DeviceArena arena_;
+  Profiler prof_;
   int launches_ = 0;
   spo::FftPlan plan_z_{}, plan_r_{}, plan_x_{}, plan_y_{}, plan_zs_{}, plan_phi_{};
   V *tw_z_ = nullptr, *tw_r_ = nullptr, *tw_x_ = nullptr, *tw_y_ = nullptr, *tw_zs_ = nullptr, *tw_phi_ = nullptr;
@@ -732,6 +831,35 @@ int spo_site_column(spo_handle* h, int ixy, double* out) {
 
 int spo_apply_stage(spo_handle* h, int stage, int half_step) {
   return guarded(h, [&] { h->impl->apply_stage(stage, half_step != 0); });
+}
+
+int spo_set_stream(spo_handle* h, void* cuda_stream) {
+  return guarded(h, [&] { h->impl->set_stream(static_cast<cudaStream_t>(cuda_stream)); });
+}
+
+int spo_profile(spo_handle* h, int enable) {
+  return guarded(h, [&] { h->impl->profile(enable != 0); });
+}
+
+int spo_profile_count(const spo_handle* h, int* n) {
+  if (!h || !n) return SPO_ERR_INVALID;
+  *n = static_cast<int>(h->impl->records().size());
+  return SPO_OK;
+}
+
+int spo_profile_entry(const spo_handle* h, int i, char* name, int name_len, double* total_ms, int* launches,
+                      double* bytes_per_launch) {
+  if (!h) return SPO_ERR_INVALID;
+  const auto& r = h->impl->records();
+  if (i < 0 || i >= static_cast<int>(r.size())) return SPO_ERR_INVALID;
+  if (name && name_len > 0) {
+    std::strncpy(name, r[i].name.c_str(), static_cast<std::size_t>(name_len) - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (total_ms) *total_ms = r[i].ms;
+  if (launches) *launches = r[i].launches;
+  if (bytes_per_launch) *bytes_per_launch = r[i].bytes;
+  return SPO_OK;
 }
 
 int spo_device_bytes(const spo_handle* h, unsigned long long* bytes) {

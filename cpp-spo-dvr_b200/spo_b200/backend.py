@@ -150,6 +150,26 @@ class B200Backend:
     def apply_stage(self, stage: int, half: bool = False) -> None:
         self._check(self._lib.spo_apply_stage(self._h, int(stage), 1 if half else 0))
 
+    def set_stream(self, cuda_stream: int | None) -> None:
+        """Run on the caller's cudaStream_t (an integer handle, e.g. torch.cuda.Stream().cuda_stream)."""
+        self._check(self._lib.spo_set_stream(self._h, ctypes.c_void_p(cuda_stream or 0)))
+
+    def profile(self, enable: bool) -> None:
+        self._check(self._lib.spo_profile(self._h, 1 if enable else 0))
+
+    def profile_records(self) -> list[dict]:
+        n = ctypes.c_int()
+        self._check(self._lib.spo_profile_count(self._h, ctypes.byref(n)))
+        out = []
+        for i in range(n.value):
+            name = ctypes.create_string_buffer(64)
+            ms, launches, nbytes = ctypes.c_double(), ctypes.c_int(), ctypes.c_double()
+            self._check(self._lib.spo_profile_entry(self._h, i, name, 64, ctypes.byref(ms), ctypes.byref(launches),
+                                                    ctypes.byref(nbytes)))
+            out.append({"name": name.value.decode(), "ms": ms.value, "launches": launches.value,
+                        "bytes_per_launch": nbytes.value})
+        return out
+
     def device_bytes(self) -> int:
         v = ctypes.c_ulonglong()
         self._check(self._lib.spo_device_bytes(self._h, ctypes.byref(v)))

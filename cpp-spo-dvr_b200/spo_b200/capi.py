@@ -25,8 +25,8 @@ PRECISION_FP64, PRECISION_MIXED = 0, 1
 EXPORTS = [
     "spo_version", "spo_last_error", "spo_create", "spo_destroy", "spo_propagate_analysis_step",
     "spo_upload_state", "spo_download_state", "spo_get_specular", "spo_get_z_plane",
-    "spo_block_densities", "spo_site_column", "spo_apply_stage", "spo_device_bytes",
-    "spo_last_launch_count",
+    "spo_block_densities", "spo_site_column", "spo_apply_stage", "spo_set_stream", "spo_profile",
+    "spo_profile_count", "spo_profile_entry", "spo_device_bytes", "spo_last_launch_count",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -84,6 +84,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.spo_block_densities.argtypes = [h, _dp]
     lib.spo_site_column.argtypes = [h, ctypes.c_int, _dp]
     lib.spo_apply_stage.argtypes = [h, ctypes.c_int, ctypes.c_int]
+    lib.spo_set_stream.argtypes = [h, ctypes.c_void_p]
+    lib.spo_profile.argtypes = [h, ctypes.c_int]
+    lib.spo_profile_count.argtypes = [h, _ip]
+    lib.spo_profile_entry.argtypes = [h, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp, _ip, _dp]
     lib.spo_device_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_ulonglong)]
     lib.spo_last_launch_count.argtypes = [h, _ip]
     for name in EXPORTS:

@@ -156,6 +156,24 @@ enum spo_stage {
 /* Applies one operator to the resident state, with the full (half_step = 0) or half (1) step's factors. */
 int spo_apply_stage(spo_handle* h, int stage, int half_step);
 
+/* Runs the handle's work on the caller's CUDA stream (a cudaStream_t of the handle's device, passed
+ * as void*), e.g. to bracket it with the caller's CUDA events; NULL returns to the handle's own stream. */
+int spo_set_stream(spo_handle* h, void* cuda_stream);
+
+/* Per-kernel timing: with enable != 0 every kernel launch of the following calls is bracketed by
+ * CUDA events on the launching stream and its duration added to a per-kernel record (reset by
+ * each spo_profile call). */
+int spo_profile(spo_handle* h, int enable);
+
+/* Number of per-kernel records. */
+int spo_profile_count(const spo_handle* h, int* n);
+
+/* Record i: kernel name (NUL-terminated, truncated to name_len), summed duration (ms), launches,
+ * and the algorithmic bytes one launch must move (its minimal HBM traffic: state read + written
+ * once, plus the exp(iV dt) table read once by the potential kernel). */
+int spo_profile_entry(const spo_handle* h, int i, char* name, int name_len, double* total_ms, int* launches,
+                      double* bytes_per_launch);
+
 /* Bytes of device memory the handle holds. */
 int spo_device_bytes(const spo_handle* h, unsigned long long* bytes);
 

@@ -15,8 +15,8 @@
 //       and, at the end, psi and the block densities. --stages additionally applies each operator
 //       of one full sub-step once to the initial state (specular, T_Zr, T_xy, V) and records the
 //       state after each.
-//   spo_ref_tool time INPUT.json [--analysis-steps K] [--random SEED]
-//       Times K calls of CpuBackend::propagate_analysis_step after one warm-up call; prints JSON.
+//   spo_ref_tool time INPUT.json [--analysis-steps K] [--warmup W] [--random SEED]
+//       Times K calls of CpuBackend::propagate_analysis_step after W warm-up calls; prints JSON.
 #include <omp.h>
 
 #include <chrono>
@@ -93,6 +93,7 @@ struct Options {
   fs::path out;
   std::optional<std::uint64_t> random_seed;
   int analysis_steps = 1;
+  int warmup = 1;
   bool stages = false;
   bool dump_psi = true;
 };
@@ -112,6 +113,7 @@ Options parse(int argc, char** argv) {
     const std::string a = argv[i];
     if (a == "--random" && i + 1 < argc) o.random_seed = std::stoull(argv[++i]);
     else if (a == "--analysis-steps" && i + 1 < argc) o.analysis_steps = std::stoi(argv[++i]);
+    else if (a == "--warmup" && i + 1 < argc) o.warmup = std::stoi(argv[++i]);
     else if (a == "--stages") o.stages = true;
     else if (a == "--no-psi") o.dump_psi = false;
     else throw std::invalid_argument("unknown option " + a);
@@ -398,7 +400,7 @@ int run_time(const Options& o) {
       fill_lcg(psi.scattering.values, *o.random_seed);
       fill_lcg(psi.specular.values, *o.random_seed + 1);
     });
-  backend->propagate_analysis_step();  // warm-up
+  for (int w = 0; w < o.warmup; ++w) backend->propagate_analysis_step();
   const auto t0 = std::chrono::steady_clock::now();
   for (int a = 0; a < o.analysis_steps; ++a) backend->propagate_analysis_step();
   const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
