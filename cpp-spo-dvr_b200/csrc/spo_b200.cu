@@ -18,6 +18,7 @@
 #include <complex>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -875,3 +876,67 @@ int spo_last_launch_count(const spo_handle* h, int* launches) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// spo_block_densities_noalloc: the block-density kernel with its per-block sums in a file-scope
+// device array instead of a handle's allocation (see include/spo_b200.h for who needs this).
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+// Per-block sums of every call (SPO_NOALLOC_MAX_BLOCKS doubles, 512 KiB per device). In host code
+// this name is only a host-side stand-in for the symbol: its device address comes from
+// cudaGetSymbolAddress, looked up once per device.
+__device__ __align__(256) double g_noalloc_density_scratch[SPO_NOALLOC_MAX_BLOCKS];
+
+constexpr int kMaxDevices = 64;
+std::once_flag g_noalloc_once[kMaxDevices];
+double* g_noalloc_ptr[kMaxDevices] = {};
+cudaError_t g_noalloc_status[kMaxDevices] = {};
+
+// The array's address on the current device (first call per device: the lookup, with that device current).
+double* noalloc_scratch(int device) {
+  std::call_once(g_noalloc_once[device], [device] {
+    void* p = nullptr;
+    g_noalloc_status[device] = cudaGetSymbolAddress(&p, g_noalloc_density_scratch);
+    g_noalloc_ptr[device] = static_cast<double*>(p);
+  });
+  check_cuda(g_noalloc_status[device], "cudaGetSymbolAddress(g_noalloc_density_scratch)");
+  return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+extern "C" int spo_block_densities_noalloc(const void* psi_device, int precision, long long n_blocks,
+                                           long long block_size, double* out_host, void* cuda_stream) {
+  try {
+    require(psi_device != nullptr && out_host != nullptr, "spo_block_densities_noalloc: null pointer");
+    require(precision == SPO_PRECISION_FP64 || precision == SPO_PRECISION_MIXED,
+            "spo_block_densities_noalloc: unknown precision");
+    require(n_blocks > 0 && block_size > 0, "spo_block_densities_noalloc: n_blocks and block_size must be positive");
+    require(n_blocks <= SPO_NOALLOC_MAX_BLOCKS,
+            "spo_block_densities_noalloc: n_blocks = " + std::to_string(n_blocks) + " exceeds SPO_NOALLOC_MAX_BLOCKS = " +
+                std::to_string(SPO_NOALLOC_MAX_BLOCKS));
+    int device = 0;
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    require(device >= 0 && device < kMaxDevices, "spo_block_densities_noalloc: device ordinal out of range");
+    double* scratch = noalloc_scratch(device);
+    const auto stream = static_cast<cudaStream_t>(cuda_stream);
+    if (precision == SPO_PRECISION_FP64)
+      spo::block_density_kernel<double><<<static_cast<unsigned>(n_blocks), 256, 0, stream>>>(
+          static_cast<const double2*>(psi_device), block_size, scratch);
+    else
+      spo::block_density_kernel<float><<<static_cast<unsigned>(n_blocks), 256, 0, stream>>>(
+          static_cast<const float2*>(psi_device), block_size, scratch);
+    check_cuda(cudaGetLastError(), "block_density_kernel launch");
+    check_cuda(cudaMemcpyAsync(out_host, scratch, sizeof(double) * n_blocks, cudaMemcpyDeviceToHost, stream),
+               "block densities copy");
+    check_cuda(cudaStreamSynchronize(stream), "spo_block_densities_noalloc");
+    return SPO_OK;
+  } catch (const SpoError& e) {
+    g_create_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return SPO_ERR_DEVICE;
+  }
+}

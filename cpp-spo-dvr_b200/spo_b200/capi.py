@@ -27,7 +27,9 @@ EXPORTS = [
     "spo_upload_state", "spo_download_state", "spo_get_specular", "spo_get_z_plane",
     "spo_block_densities", "spo_site_column", "spo_apply_stage", "spo_set_stream", "spo_profile",
     "spo_profile_count", "spo_profile_entry", "spo_device_bytes", "spo_last_launch_count",
+    "spo_block_densities_noalloc",
 ]
+NOALLOC_MAX_BLOCKS = 65536
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -89,6 +91,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.spo_profile_count.argtypes = [h, _ip]
     lib.spo_profile_entry.argtypes = [h, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp, _ip, _dp]
     lib.spo_device_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.spo_block_densities_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong,
+                                                _dp, ctypes.c_void_p]
     lib.spo_last_launch_count.argtypes = [h, _ip]
     for name in EXPORTS:
         if name not in ("spo_version", "spo_last_error"):

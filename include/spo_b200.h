@@ -180,6 +180,35 @@ int spo_device_bytes(const spo_handle* h, unsigned long long* bytes);
 /* Number of kernel launches the last spo_propagate_analysis_step issued. */
 int spo_last_launch_count(const spo_handle* h, int* launches);
 
+/* ---------------------------------------------------------------------------------------------
+ * Block densities without any device allocation.
+ *
+ * No counterpart in the reference: an addition for callers that cannot allocate device memory
+ * themselves. A host program whose device memory is owned by a pool allocator (a framework's caching
+ * allocator, an application arena sized at start-up) must not call cudaMalloc/cudaFree behind the
+ * pool's back: a cudaMalloc can fail while the pool holds the free memory, and cudaFree synchronises
+ * the whole device. spo_create allocates, so such callers keep the wave packet in their own buffers
+ * and call this entry point on it.
+ *
+ * psi_device: n_blocks consecutive blocks of block_size complex values in device memory (complex128
+ * when precision is SPO_PRECISION_FP64, complex64 when SPO_PRECISION_MIXED), i.e. the wave packet
+ * in the layout of this library with block_size = n_rot*nx*ny and n_blocks = nz*nr. out_host: n_blocks
+ * doubles in host memory, sum |psi|^2 of each block in FP64 with the fixed summation order of
+ * spo_block_densities. cuda_stream: a cudaStream_t of the current device (NULL: the legacy default
+ * stream); the call returns after the results are in out_host.
+ *
+ * Limit: n_blocks <= SPO_NOALLOC_MAX_BLOCKS (larger values are refused with SPO_ERR_INVALID). The
+ * per-block sums go through a fixed scratch array of SPO_NOALLOC_MAX_BLOCKS doubles (512 KiB) that
+ * every GPU which loads the library holds until the process exits. All calls share that array: calls
+ * that overlap on the GPU (different streams or threads at the same time) race on it. Every element a
+ * call reads is written by the same call first, so nothing needs clearing between calls. The first
+ * call on a device looks up the array's device address for that device, with it current; make that
+ * first call before any stream capture. Messages of refused calls: spo_last_error(NULL).
+ * --------------------------------------------------------------------------------------------- */
+#define SPO_NOALLOC_MAX_BLOCKS 65536
+int spo_block_densities_noalloc(const void* psi_device, int precision, long long n_blocks, long long block_size,
+                                double* out_host, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
