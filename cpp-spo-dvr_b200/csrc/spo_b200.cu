@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -25,6 +26,7 @@
 
 #include "../../include/spo_b200.h"
 #include "spo_kernels.cuh"
+#include "spo_regfft.cuh"
 
 namespace {
 
@@ -130,6 +132,142 @@ struct Sizes {
   long long n_expia() const { return static_cast<long long>(nzp) * nr * n_rep * nt * nphi; }
 };
 
+
+// ---------------------------------------------------------------------------------------------
+// Launchers of the register-DFT kernels for the sizes they are instantiated for. Each returns
+// false for other sizes; the caller then uses the general shared-memory Stockham kernels.
+// ---------------------------------------------------------------------------------------------
+template <typename T, int N1, int N2>
+bool launch_axis2_n(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
+  constexpr int NS = N1 > N2 ? N1 : N2;
+  constexpr int TB = NS <= 8 ? 32 : 16;
+  constexpr int N = N1 * N2;
+  const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(N) * TB + 2 * N);
+  static bool configured = false;
+  if (!configured) {
+    check_cuda(cudaFuncSetAttribute(spo::axis2_kernel<T, N1, N2, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)),
+               "axis2 smem");
+    configured = true;
+  }
+  const dim3 grid(static_cast<unsigned>((a.inner + TB - 1) / TB), static_cast<unsigned>(outer));
+  spo::axis2_kernel<T, N1, N2, TB><<<grid, TB * NS, smem, stream>>>(a);
+  return true;
+}
+
+template <typename T>
+bool launch_axis2(int n, const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
+  switch (n) {
+    case 24: return launch_axis2_n<T, 6, 4>(a, outer, stream);
+    case 32: return launch_axis2_n<T, 8, 4>(a, outer, stream);
+    case 40: return launch_axis2_n<T, 8, 5>(a, outer, stream);
+    case 48: return launch_axis2_n<T, 8, 6>(a, outer, stream);
+    case 56: return launch_axis2_n<T, 8, 7>(a, outer, stream);
+    case 64: return launch_axis2_n<T, 8, 8>(a, outer, stream);
+    case 80: return launch_axis2_n<T, 10, 8>(a, outer, stream);
+    case 96: return launch_axis2_n<T, 12, 8>(a, outer, stream);
+    case 112: return launch_axis2_n<T, 16, 7>(a, outer, stream);
+    case 128: return launch_axis2_n<T, 16, 8>(a, outer, stream);
+    case 160: return launch_axis2_n<T, 16, 10>(a, outer, stream);
+    case 176: return launch_axis2_n<T, 16, 11>(a, outer, stream);
+    case 192: return launch_axis2_n<T, 16, 12>(a, outer, stream);
+    case 224: return launch_axis2_n<T, 16, 14>(a, outer, stream);
+    case 256: return launch_axis2_n<T, 16, 16>(a, outer, stream);
+    default: return false;
+  }
+}
+bool axis2_supported(int n) {
+  switch (n) {
+    case 24: case 32: case 40: case 48: case 56: case 64: case 80: case 96: case 112: case 128: case 160: case 176:
+    case 192: case 224: case 256: return true;
+    default: return false;
+  }
+}
+
+template <typename T, int NX, int NY>
+void launch_xy2_n(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream) {
+  constexpr int NS = NX > NY ? NX : NY;
+  constexpr int TB = NS <= 8 ? 32 : 16;
+  const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(NX * NY) * TB + NX * NY);
+  static bool configured = false;
+  if (!configured) {
+    check_cuda(cudaFuncSetAttribute(spo::xy2_kernel<T, NX, NY, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)),
+               "xy2 smem");
+    configured = true;
+  }
+  const dim3 grid(static_cast<unsigned>((a.n_rot + TB - 1) / TB), static_cast<unsigned>(n_zr));
+  spo::xy2_kernel<T, NX, NY, TB><<<grid, TB * NS, smem, stream>>>(a);
+}
+
+template <typename T>
+bool launch_xy2(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream) {
+  if (a.nx != a.ny) return false;
+  switch (a.nx) {
+    case 2: launch_xy2_n<T, 2, 2>(a, n_zr, stream); return true;
+    case 4: launch_xy2_n<T, 4, 4>(a, n_zr, stream); return true;
+    case 6: launch_xy2_n<T, 6, 6>(a, n_zr, stream); return true;
+    case 8: launch_xy2_n<T, 8, 8>(a, n_zr, stream); return true;
+    case 12: launch_xy2_n<T, 12, 12>(a, n_zr, stream); return true;
+    case 16: launch_xy2_n<T, 16, 16>(a, n_zr, stream); return true;
+    default: return false;
+  }
+}
+
+// Shared memory of potential2_kernel<T, NPHI, CB>.
+template <typename T>
+std::size_t pot2_smem(int cb, int n_rot, int nt, int nphi, long long n_xy) {
+  return sizeof(spo::Vec<T>) * (static_cast<std::size_t>(cb) * n_rot + static_cast<std::size_t>(cb) * nt * (nphi + 1) +
+                                n_xy + 32) +
+         sizeof(T) * static_cast<std::size_t>(nt) * n_rot;
+}
+
+template <typename T, int NPHI, int CB>
+void launch_pot2_n(const spo::Pot2Args<T>& a, unsigned blocks, std::size_t smem, cudaStream_t stream) {
+  static bool configured = false;
+  if (!configured) {
+    int dev = 0, optin = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "smem attribute");
+    check_cuda(cudaFuncSetAttribute(spo::potential2_kernel<T, NPHI, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    optin),
+               "potential2 smem");
+    configured = true;
+  }
+  spo::potential2_kernel<T, NPHI, CB><<<blocks, 128, smem, stream>>>(a);
+}
+
+template <typename T, int NPHI>
+void launch_pot2_phi(const spo::Pot2Args<T>& a, unsigned blocks, std::size_t smem, cudaStream_t stream) {
+  switch (a.cb) {
+    case 32: launch_pot2_n<T, NPHI, 32>(a, blocks, smem, stream); break;
+    case 8: launch_pot2_n<T, NPHI, 8>(a, blocks, smem, stream); break;
+    default: launch_pot2_n<T, NPHI, 4>(a, blocks, smem, stream); break;
+  }
+}
+
+template <typename T>
+void launch_pot2(int nphi, const spo::Pot2Args<T>& a, unsigned blocks, std::size_t smem, cudaStream_t stream) {
+  switch (nphi) {
+    case 6: launch_pot2_phi<T, 6>(a, blocks, smem, stream); break;
+    case 8: launch_pot2_phi<T, 8>(a, blocks, smem, stream); break;
+    case 10: launch_pot2_phi<T, 10>(a, blocks, smem, stream); break;
+    case 12: launch_pot2_phi<T, 12>(a, blocks, smem, stream); break;
+    case 16: launch_pot2_phi<T, 16>(a, blocks, smem, stream); break;
+    case 20: launch_pot2_phi<T, 20>(a, blocks, smem, stream); break;
+    case 24: launch_pot2_phi<T, 24>(a, blocks, smem, stream); break;
+    case 30: launch_pot2_phi<T, 30>(a, blocks, smem, stream); break;
+    case 32: launch_pot2_phi<T, 32>(a, blocks, smem, stream); break;
+    default: break;
+  }
+}
+bool pot2_phi_supported(int nphi) {
+  switch (nphi) {
+    case 6: case 8: case 10: case 12: case 16: case 20: case 24: case 30: case 32: return true;
+    default: return false;
+  }
+}
+
 // Per-kernel CUDA-event timing record.
 struct KernelRecord {
   std::string name;
@@ -214,6 +352,9 @@ class StepBase {
   virtual void block_densities(double* out) = 0;
   virtual void site_column(int ixy, double* out) = 0;
   virtual void apply_stage(int stage, bool half) = 0;
+  virtual void analysis_setup(const spo_analysis_desc& d) = 0;
+  virtual void bk(double time, bool fixed, int surface_index, bool accumulate, double* out) = 0;
+  virtual void s_sums(double* out) = 0;
   virtual unsigned long long bytes() const = 0;
   virtual int launches() const = 0;
   virtual void set_stream(cudaStream_t s) = 0;
@@ -301,6 +442,93 @@ class Step final : public StepBase {
     prof_.resolve();
   }
 
+  void analysis_setup(const spo_analysis_desc& d) override {
+    require(d.n_v > 0 && d.n_rotation > 0 && d.n_diffraction > 0 && d.n_energies >= 0, "analysis sizes invalid");
+    require(d.iz_analysis >= 0 && d.iz_analysis < s_.nz, "iz_analysis out of range");
+    require(d.initial_state >= 0 && d.initial_state < d.n_rotation * d.n_diffraction, "initial_state out of range");
+    require(d.j_in >= 0 && d.j_in <= d.j_max_gas, "j_in out of range");
+    an_ = d;
+    const std::vector<int> rot = int_array(d.rotation_index, d.n_rotation, "rotation_index");
+    const std::vector<int> rj = int_array(d.rotation_j, d.n_rotation, "rotation_j");
+    const std::vector<int> cx = int_array(d.channel_ix, d.n_diffraction, "channel_ix");
+    const std::vector<int> cy = int_array(d.channel_iy, d.n_diffraction, "channel_iy");
+    for (int i = 0; i < d.n_rotation; ++i)
+      require(rot[i] >= 0 && rot[i] < s_.n_rot && rj[i] >= 0 && rj[i] <= d.j_max_gas, "analysed rotation out of range");
+    for (int i = 0; i < d.n_diffraction; ++i)
+      require(cx[i] >= 0 && cx[i] < s_.nx && cy[i] >= 0 && cy[i] < s_.ny, "diffraction channel out of range");
+    const std::size_t n_phi = static_cast<std::size_t>(s_.nr) * (d.j_max_gas + 1) * d.n_v;
+    an_rot_ = upload_int(rot);
+    an_j_ = upload_int(rj);
+    an_cx_ = upload_int(cx);
+    an_cy_ = upload_int(cy);
+    an_phi_ = upload_f64(real_array(d.phi_vj, n_phi, "phi_vj"));
+    an_energies_ = upload_f64(d.n_energies > 0 ? real_array(d.energies_hartree, d.n_energies, "energies_hartree")
+                                               : std::vector<double>(1, 0.0));
+    an_twx_ = upload_c128(twiddles(s_.nx));
+    an_twy_ = upload_c128(twiddles(s_.ny));
+    an_shift_ = upload_c128(shift_host_);
+    const long long n = static_cast<long long>(d.n_rotation) * d.n_diffraction * d.n_v;
+    an_bk_ = dev<double2>(n);
+    an_sums_ = dev<double2>(std::max<long long>(n * d.n_energies, 1));
+    check_cuda(cudaMemsetAsync(an_sums_, 0, sizeof(double2) * std::max<long long>(n * d.n_energies, 1), stream_),
+               "zero S sums");
+    check_cuda(cudaStreamSynchronize(stream_), "analysis_setup");
+    an_ready_ = true;
+  }
+
+  void bk(double time, bool fixed, int surface_index, bool accumulate, double* out) override {
+    require(an_ready_, "spo_analysis_setup was not called");
+    require(!fixed || (surface_index >= 0 && surface_index < s_.nzs), "surface_index out of range");
+    spo::BkArgs<T> a{};
+    a.psi = psi_;
+    a.n_rot = s_.n_rot;
+    a.nx = s_.nx;
+    a.ny = s_.ny;
+    a.nr = s_.nr;
+    a.iz_analysis = an_.iz_analysis;
+    a.n_v = an_.n_v;
+    a.n_rotation = an_.n_rotation;
+    a.n_diffraction = an_.n_diffraction;
+    a.j_max_gas = an_.j_max_gas;
+    a.rotation_index = an_rot_;
+    a.rotation_j = an_j_;
+    a.channel_ix = an_cx_;
+    a.channel_iy = an_cy_;
+    a.phi_vj = an_phi_;
+    a.shift = an_shift_;
+    a.dr = an_.dr;
+    a.xy_scale = an_.xy_scale;
+    a.px = plan_x_;
+    a.py = plan_y_;
+    a.twx = an_twx_;
+    a.twy = an_twy_;
+    a.bk = an_bk_;
+    const std::size_t smem = sizeof(double2) * (2 * s_.n_xy() + s_.nx + s_.ny);
+    spo::bk_kernel<T><<<an_.n_v * an_.n_rotation, 256, smem, stream_>>>(a);
+    const int n_states = an_.n_rotation * an_.n_diffraction;
+    if (fixed)
+      spo::bk_specular_kernel<T><<<(an_.n_v + 127) / 128, 128, 0, stream_>>>(
+          chi_, s_.nr, surface_index, an_phi_, an_.j_max_gas, an_.j_in, an_.n_v, n_states, an_.initial_state, an_.dr,
+          an_bk_);
+    const int n = n_states * an_.n_v;
+    if (accumulate && an_.n_energies > 0)
+      spo::s_matrix_add_kernel<<<std::min<long long>((static_cast<long long>(n) * an_.n_energies + 255) / 256, 1184),
+                                 256, 0, stream_>>>(an_bk_, n, an_energies_, an_.n_energies, time,
+                                                    an_.analysis_time_step, an_sums_);
+    check_cuda(cudaGetLastError(), "bk launch");
+    if (out)
+      check_cuda(cudaMemcpyAsync(out, an_bk_, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream_), "bk copy");
+    check_cuda(cudaStreamSynchronize(stream_), "bk");
+  }
+
+  void s_sums(double* out) override {
+    require(an_ready_, "spo_analysis_setup was not called");
+    const long long n = static_cast<long long>(an_.n_rotation) * an_.n_diffraction * an_.n_v * an_.n_energies;
+    if (n > 0)
+      check_cuda(cudaMemcpyAsync(out, an_sums_, sizeof(double2) * n, cudaMemcpyDeviceToHost, stream_), "S copy");
+    check_cuda(cudaStreamSynchronize(stream_), "s_sums");
+  }
+
   unsigned long long bytes() const override { return arena_.bytes(); }
   int launches() const override { return launches_; }
   void set_stream(cudaStream_t s) override { stream_ = s ? s : own_stream_; }
@@ -330,10 +558,23 @@ class Step final : public StepBase {
   // T_Z and T_r of the scattering wave.
   void kinetic_zr(bool half) {
     const double b = 2.0 * sizeof(V) * s_.n_psi();
-    axis("kinetic_z", b, psi_, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, spo::kFactorAxis,
-         spo::kFwdFactorInv, nullptr);
-    axis("kinetic_r", b, psi_, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, spo::kFactorAxis,
-         spo::kFwdFactorInv, nullptr);
+    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_);
+    axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_);
+  }
+
+  // A kinetic axis pass over psi: the register-DFT kernel for its length when instantiated, else the
+  // general Stockham kernel.
+  void axis_psi(const char* name, double bytes, long long outer, const spo::FftPlan& plan, const V* tw,
+                long long inner, const V* factor) {
+    if (use_v2_ && axis2_supported(plan.n)) {
+      spo::Axis2Args<T> a{psi_, inner, factor, tw};
+      prof_.begin(stream_);
+      launch_axis2<T>(plan.n, a, outer, stream_);
+      prof_.end(stream_, name, bytes);
+      ++launches_;
+      return;
+    }
+    axis(name, bytes, psi_, outer, plan, tw, inner, factor, spo::kFactorAxis, spo::kFwdFactorInv, nullptr);
   }
 
   // T_xy, optionally with the gas-phase potential step fused.
@@ -358,7 +599,7 @@ class Step final : public StepBase {
     x.gas_step = gas_step_;
     const dim3 xg((s_.n_rot + xy_tb_ - 1) / xy_tb_, static_cast<unsigned>(s_.n_zr()));
     prof_.begin(stream_);
-    spo::xy_pass_kernel<T><<<xg, 256, xy_smem_, stream_>>>(x);
+    if (!(use_v2_ && launch_xy2<T>(x, s_.n_zr(), stream_))) spo::xy_pass_kernel<T><<<xg, 256, xy_smem_, stream_>>>(x);
     prof_.end(stream_, "kinetic_xy", 2.0 * sizeof(V) * s_.n_psi());
     ++launches_;
   }
@@ -376,7 +617,10 @@ class Step final : public StepBase {
   void interaction() {
     if (s_.nzp == 0) return;
     prof_.begin(stream_);
-    spo::potential_kernel<T><<<static_cast<unsigned>(s_.nzp) * s_.nr, 256, pot_smem_, stream_>>>(pot_);
+    if (use_v2_ && pot2_cb_ > 0)
+      launch_pot2<T>(s_.nphi, pot2_, static_cast<unsigned>(s_.nzp) * s_.nr, pot2_smem_, stream_);
+    else
+      spo::potential_kernel<T><<<static_cast<unsigned>(s_.nzp) * s_.nr, 256, pot_smem_, stream_>>>(pot_);
     prof_.end(stream_, "potential",
               sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia())));
     ++launches_;
@@ -431,6 +675,16 @@ class Step final : public StepBase {
     std::vector<T> h(v.begin(), v.end());
     T* d = dev<T>(v.size());
     check_cuda(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice), "upload table");
+    return d;
+  }
+  double* upload_f64(const std::vector<double>& v) {
+    double* d = dev<double>(v.size());
+    check_cuda(cudaMemcpy(d, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice), "upload table");
+    return d;
+  }
+  double2* upload_c128(const std::vector<cplx>& v) {
+    double2* d = dev<double2>(v.size());
+    check_cuda(cudaMemcpy(d, v.data(), sizeof(double2) * v.size(), cudaMemcpyHostToDevice), "upload table");
     return d;
   }
   int* upload_int(const std::vector<int>& v) {
@@ -512,6 +766,7 @@ class Step final : public StepBase {
     opt_z_ = upload_real(opt_z);
 
     const std::vector<cplx> shf = complex_array(d.shift_forward, nxy, "shift_forward");
+    shift_host_ = shf;
     const bool shift = std::any_of(shf.begin(), shf.end(), [](const cplx& c) { return c.real() != 1.0 || c.imag() != 0.0; });
     if (shift) {
       shift_f_ = upload_complex(shf);
@@ -635,6 +890,38 @@ class Step final : public StepBase {
     pot_.expia = expia_;
     pot_.rep_of = upload_int(rep);
     pot_.phi_map = upload_int(phi_map);
+
+    // The register-phi potential kernel: CB columns per chunk with CB * ntheta lines <= 128 threads and
+    // at most ~110 KiB of shared memory (two blocks per SM), when nphi has an instantiation.
+    pot2_cb_ = 0;
+    if (pot2_phi_supported(s.nphi) && s.nt <= 32) {
+      for (const int cb : {32, 8, 4}) {
+        if (cb * s.nt > 128 || cb > nxy * 2) continue;
+        const std::size_t need = pot2_smem<T>(cb, s.n_rot, s.nt, s.nphi, nxy);
+        if (need <= std::min<std::size_t>(smem_optin, 110u << 10) || (cb == 4 && need <= static_cast<std::size_t>(smem_optin))) {
+          pot2_cb_ = cb;
+          pot2_smem_ = need;
+          break;
+        }
+      }
+    }
+    if (pot2_cb_ > 0) {
+      std::vector<double> leg_t(legendre.size());
+      for (int b = 0; b < s.n_blocks; ++b)
+        for (int t = 0; t < s.nt; ++t)
+          for (int j = 0; j < size[b]; ++j)
+            leg_t[offset[b] + j * s.nt + t] = legendre[offset[b] + t * size[b] + j];
+      pot2_.p = pot_;
+      pot2_.legendre_t = upload_real(leg_t);
+      pot2_.cb = pot2_cb_;
+      bool identity = s.n_rep == nxy;
+      for (long long ixy = 0; ixy < nxy && identity; ++ixy) {
+        identity = rep[ixy] == ixy;
+        for (int p = 0; p < s.nphi && identity; ++p) identity = phi_map[ixy * s.nphi + p] == p;
+      }
+      pot2_.identity_maps = identity ? 1 : 0;
+    }
+    if (const char* env = std::getenv("SPO_B200_KERNELS")) use_v2_ = std::string(env) != "v1";
     check_cuda(cudaStreamSynchronize(stream_), "set-up");
   }
 
@@ -686,6 +973,17 @@ class Step final : public StepBase {
   int xy_tb_ = 1;
   std::size_t xy_smem_ = 0, pot_smem_ = 0;
   spo::PotArgs<T> pot_{};
+  spo::Pot2Args<T> pot2_{};
+  int pot2_cb_ = 0;
+  std::size_t pot2_smem_ = 0;
+  bool use_v2_ = true;  // register-DFT kernels where instantiated (SPO_B200_KERNELS=v1: the general kernels)
+  // Asymptotic analysis (FP64).
+  std::vector<cplx> shift_host_;
+  spo_analysis_desc an_{};
+  bool an_ready_ = false;
+  int *an_rot_ = nullptr, *an_j_ = nullptr, *an_cx_ = nullptr, *an_cy_ = nullptr;
+  double *an_phi_ = nullptr, *an_energies_ = nullptr;
+  double2 *an_twx_ = nullptr, *an_twy_ = nullptr, *an_shift_ = nullptr, *an_bk_ = nullptr, *an_sums_ = nullptr;
 };
 
 Sizes sizes_of(const spo_desc& d) {
@@ -827,6 +1125,25 @@ int spo_site_column(spo_handle* h, int ixy, double* out) {
   return guarded(h, [&] {
     require(out != nullptr, "out is null");
     h->impl->site_column(ixy, out);
+  });
+}
+
+int spo_analysis_setup(spo_handle* h, const spo_analysis_desc* d) {
+  return guarded(h, [&] {
+    require(d != nullptr, "analysis descriptor is null");
+    h->impl->analysis_setup(*d);
+  });
+}
+
+int spo_bk_coefficients(spo_handle* h, double time, int surface_fixed, int surface_index, int accumulate,
+                        double* bk_out) {
+  return guarded(h, [&] { h->impl->bk(time, surface_fixed != 0, surface_index, accumulate != 0, bk_out); });
+}
+
+int spo_s_matrix_sums(spo_handle* h, double* out) {
+  return guarded(h, [&] {
+    require(out != nullptr, "out is null");
+    h->impl->s_sums(out);
   });
 }
 

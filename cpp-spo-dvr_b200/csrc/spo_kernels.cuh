@@ -21,21 +21,23 @@ template <> struct VecOf<double> { using type = double2; };
 template <> struct VecOf<float> { using type = float2; };
 template <typename T> using Vec = typename VecOf<T>::type;
 
-template <typename V> __device__ __forceinline__ V cmake(decltype(V::x) re, decltype(V::x) im) {
+#define SPO_HD __host__ __device__ __forceinline__
+
+template <typename V> SPO_HD V cmake(decltype(V::x) re, decltype(V::x) im) {
   V v;
   v.x = re;
   v.y = im;
   return v;
 }
-template <typename V> __device__ __forceinline__ V cadd(V a, V b) { return cmake<V>(a.x + b.x, a.y + b.y); }
-template <typename V> __device__ __forceinline__ V csub(V a, V b) { return cmake<V>(a.x - b.x, a.y - b.y); }
-template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
+template <typename V> SPO_HD V cadd(V a, V b) { return cmake<V>(a.x + b.x, a.y + b.y); }
+template <typename V> SPO_HD V csub(V a, V b) { return cmake<V>(a.x - b.x, a.y - b.y); }
+template <typename V> SPO_HD V cmul(V a, V b) {
   return cmake<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-template <typename V> __device__ __forceinline__ V cconj(V a) { return cmake<V>(a.x, -a.y); }
-template <typename V> __device__ __forceinline__ V cscale(V a, decltype(V::x) s) { return cmake<V>(a.x * s, a.y * s); }
+template <typename V> SPO_HD V cconj(V a) { return cmake<V>(a.x, -a.y); }
+template <typename V> SPO_HD V cscale(V a, decltype(V::x) s) { return cmake<V>(a.x * s, a.y * s); }
 // i * s * a for s = +1 or -1.
-template <typename V> __device__ __forceinline__ V cimul(V a, int s) {
+template <typename V> SPO_HD V cimul(V a, int s) {
   return s > 0 ? cmake<V>(-a.y, a.x) : cmake<V>(a.y, -a.x);
 }
 
@@ -517,6 +519,97 @@ __global__ void site_column_kernel(const Vec<T>* __restrict__ psi, double2* __re
     const int irot = static_cast<int>(i / n_zr);
     const Vec<T> v = psi[(izr * n_xy + ixy) * n_rot + irot];
     out[i] = make_double2(v.x, v.y);
+  }
+}
+
+// Balint-Kurti projection, one block per (v, irotana) (src/analysis/balint_kurti.cpp:53-74), FP64:
+// overlap(ixy) = sum_ir shift(ixy) psi(iz_a, ir, ixy, irot) phi_vj(ir) dr in ir order, a 2D (x, y)
+// DFT (sign -1, scale 1), the diffraction channels times xy_scale.
+template <typename T>
+struct BkArgs {
+  const Vec<T>* psi;
+  int n_rot, nx, ny, nr, iz_analysis;
+  int n_v, n_rotation, n_diffraction, j_max_gas;
+  const int* rotation_index;
+  const int* rotation_j;
+  const int* channel_ix;
+  const int* channel_iy;
+  const double* phi_vj;  // (ir, j, v)
+  const double2* shift;  // nx*ny, FP64
+  double dr, xy_scale;
+  FftPlan px, py;
+  const double2* twx;
+  const double2* twy;
+  double2* bk;           // (is, v)
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) bk_kernel(BkArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nxy = a.nx * a.ny;
+  double2* o0 = reinterpret_cast<double2*>(smem_raw);
+  double2* o1 = o0 + nxy;
+  double2* twx = o1 + nxy;
+  double2* twy = twx + a.nx;
+  const int v = blockIdx.x / a.n_rotation;
+  const int irotana = blockIdx.x % a.n_rotation;
+  const int irot = a.rotation_index[irotana];
+  const double* phi = a.phi_vj + static_cast<long long>(a.nr) * (a.rotation_j[irotana] + (a.j_max_gas + 1) * v);
+  for (int k = threadIdx.x; k < a.nx; k += blockDim.x) twx[k] = a.twx[k];
+  for (int k = threadIdx.x; k < a.ny; k += blockDim.x) twy[k] = a.twy[k];
+  const long long plane = static_cast<long long>(a.iz_analysis) * a.nr * nxy;
+  for (int ixy = threadIdx.x; ixy < nxy; ixy += blockDim.x) {
+    double2 s = make_double2(0.0, 0.0);
+    const double2 sh = a.shift[ixy];
+    for (int ir = 0; ir < a.nr; ++ir) {
+      const Vec<T> p = a.psi[((plane + static_cast<long long>(ir) * nxy) + ixy) * a.n_rot + irot];
+      const double w = phi[ir] * a.dr;
+      const double2 t = cmul(sh, make_double2(p.x, p.y));
+      s = make_double2(s.x + t.x * w, s.y + t.y * w);
+    }
+    o0[ixy] = s;
+  }
+  __syncthreads();
+  double2* cur = smem_fft(o0, o1, twy, a.py, -1, a.nx, 1, a.ny, 1);    // along y: lines ix, stride 1
+  double2* oth = cur == o0 ? o1 : o0;
+  cur = smem_fft(cur, oth, twx, a.px, -1, a.ny, a.ny, 0, a.ny);         // along x: lines iy, stride ny
+  const int n_states = a.n_rotation * a.n_diffraction;
+  for (int idif = threadIdx.x; idif < a.n_diffraction; idif += blockDim.x) {
+    const double2 c = cur[a.channel_ix[idif] * a.ny + a.channel_iy[idif]];
+    a.bk[irotana * a.n_diffraction + idif + static_cast<long long>(n_states) * v] =
+        make_double2(c.x * a.xy_scale, c.y * a.xy_scale);
+  }
+}
+
+// The initial state's coefficients from the specular wave at the fixed analysis line iz
+// (balint_kurti.cpp:76-84): sum_ir chi(ir, iz) phi_(v, jin)(ir), times dr, in ir order.
+template <typename T>
+__global__ void bk_specular_kernel(const Vec<T>* __restrict__ chi, int nr, int iz, const double* __restrict__ phi_vj,
+                                   int j_max_gas, int j_in, int n_v, int n_states, int initial_state, double dr,
+                                   double2* __restrict__ bk) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n_v) return;
+  const double* phi = phi_vj + static_cast<long long>(nr) * (j_in + (j_max_gas + 1) * v);
+  double2 s = make_double2(0.0, 0.0);
+  for (int ir = 0; ir < nr; ++ir) {
+    const Vec<T> c = chi[ir + static_cast<long long>(nr) * iz];
+    s = make_double2(s.x + c.x * phi[ir], s.y + c.y * phi[ir]);
+  }
+  bk[initial_state + static_cast<long long>(n_states) * v] = make_double2(s.x * dr, s.y * dr);
+}
+
+// S-matrix sums (s_matrix.cpp:49-56): sums(k, ien) += bk(k) exp(i E_ien t) dt_analysis, FP64.
+__global__ void s_matrix_add_kernel(const double2* __restrict__ bk, int n, const double* __restrict__ energies,
+                                    int n_energies, double time, double dt, double2* __restrict__ sums) {
+  const long long total = static_cast<long long>(n) * n_energies;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(i % n);
+    const int ien = static_cast<int>(i / n);
+    double sn, cs;
+    sincos(energies[ien] * time, &sn, &cs);
+    const double2 t = cmul(bk[k], make_double2(cs, sn));
+    sums[i] = make_double2(sums[i].x + t.x * dt, sums[i].y + t.y * dt);
   }
 }
 

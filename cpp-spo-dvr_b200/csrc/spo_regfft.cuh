@@ -1,0 +1,470 @@
+// Register-resident DFTs with compile-time sizes, and the two-level FFT passes built on them.
+//
+// A DFT of N = P Q values held in one thread's registers is split recursively (Cooley-Tukey,
+// decimation in time): P sub-DFTs of length Q over x[p + P q], twiddles w_N^(p k1), then Q DFTs of
+// length P. The base radices are 2, 4 and the odd primes 3, 5, 7, 11 (the factors of the reference's
+// FFT sizes, src/fft/fft_sizes.cpp:9-34). Every index and every twiddle is a compile-time constant:
+// the roots of unity are template constants evaluated by the compiler from cos/sin written here (a
+// Taylor polynomial on |r| <= pi/4 after an exact quadrant reduction), so the unrolled butterflies
+// are plain FMAs with immediate operands.
+#pragma once
+
+#include <type_traits>
+#include <utility>
+
+#include "spo_kernels.cuh"
+
+namespace spo {
+
+// ---------------------------------------------------------------------------------------------
+// Compile-time roots of unity
+// ---------------------------------------------------------------------------------------------
+constexpr double kHalfPi = 1.57079632679489661923132169163975144;
+
+// sin and cos of |r| <= pi/4 by their Taylor series (Horner form, terms to r^25 / 25!, below 1e-22).
+constexpr double taylor_sin(double r) {
+  const double r2 = r * r;
+  double s = 0.0;
+  for (int n = 12; n >= 1; --n) s = (1.0 - s * r2 / ((2.0 * n) * (2.0 * n + 1.0)));
+  return r * s;
+}
+constexpr double taylor_cos(double r) {
+  const double r2 = r * r;
+  double s = 0.0;
+  for (int n = 12; n >= 1; --n) s = (1.0 - s * r2 / ((2.0 * n - 1.0) * (2.0 * n)));
+  return s;
+}
+// cos and sin of 2 pi k / n: q = the nearest quarter turn, r = 2 pi k / n - q pi / 2 computed from the
+// exact integer 4k - q n, then the quarter turns applied exactly.
+constexpr long quarter_of(long k, long n) { return (8 * k + n) / (2 * n); }
+constexpr double reduced_angle(long k, long n) {
+  return kHalfPi * static_cast<double>(4 * k - quarter_of(k, n) * n) / static_cast<double>(n);
+}
+constexpr double root_cos(long k, long n) {
+  k = ((k % n) + n) % n;
+  const double r = reduced_angle(k, n);
+  switch (quarter_of(k, n) & 3) {
+    case 0: return taylor_cos(r);
+    case 1: return -taylor_sin(r);
+    case 2: return -taylor_cos(r);
+    default: return taylor_sin(r);
+  }
+}
+constexpr double root_sin(long k, long n) {
+  k = ((k % n) + n) % n;
+  const double r = reduced_angle(k, n);
+  switch (quarter_of(k, n) & 3) {
+    case 0: return taylor_sin(r);
+    case 1: return taylor_cos(r);
+    case 2: return -taylor_sin(r);
+    default: return -taylor_cos(r);
+  }
+}
+
+// exp(S 2 pi i K / N) as a compile-time constant pair.
+template <long K, long N, int S>
+struct Root {
+  static constexpr double re = root_cos(K, N);
+  static constexpr double im = S * root_sin(K, N);
+};
+
+// The compile-time value of a static_for index.
+#define SPO_CV(i) decltype(i)::value
+
+template <int B, int E, typename F>
+SPO_HD void static_for(F&& f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(f);
+  }
+}
+
+template <typename V, long K, long N, int S>
+SPO_HD V twiddle_mul(V a) {
+  constexpr long k = ((K % N) + N) % N;
+  if constexpr (k == 0) {
+    return a;
+  } else if constexpr (4 * k == N) {  // S i
+    return cimul(a, S);
+  } else if constexpr (2 * k == N) {
+    return cmake<V>(-a.x, -a.y);
+  } else if constexpr (4 * k == 3 * N) {  // -S i
+    return cimul(a, -S);
+  } else {
+    using R = decltype(V::x);
+    constexpr R c = static_cast<R>(Root<k, N, S>::re);
+    constexpr R s = static_cast<R>(Root<k, N, S>::im);
+    return cmake<V>(a.x * c - a.y * s, a.x * s + a.y * c);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Register DFT, in place, natural order in and out: x[k] <- sum_n x[n] exp(S 2 pi i n k / N)
+// ---------------------------------------------------------------------------------------------
+constexpr int first_factor(int n) {
+  if (n % 4 == 0 && n != 4) return 4;
+  for (int p : {2, 3, 5, 7, 11})
+    if (n % p == 0) return p;
+  return n;
+}
+constexpr bool supported_size(int n) {
+  while (n % 2 == 0) n /= 2;
+  for (int p : {3, 5, 7, 11})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+template <int N, int S, typename V>
+SPO_HD void rdft(V (&x)[N]) {
+  static_assert(supported_size(N), "register DFT sizes are products of 2, 3, 5, 7, 11");
+  if constexpr (N == 1) {
+  } else if constexpr (N == 2) {
+    const V a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+  } else if constexpr (N == 4) {
+    const V s02 = cadd(x[0], x[2]), d02 = csub(x[0], x[2]);
+    const V s13 = cadd(x[1], x[3]), d13 = csub(x[1], x[3]);
+    const V jd = cimul(d13, S);
+    x[0] = cadd(s02, s13);
+    x[1] = cadd(d02, jd);
+    x[2] = csub(s02, s13);
+    x[3] = csub(d02, jd);
+  } else if constexpr (N == 3 || N == 5 || N == 7 || N == 11) {
+    // Odd prime: pairs (t, N - t) share the real part of the root and have opposite imaginary parts.
+    using R = decltype(V::x);
+    constexpr int H = N / 2;
+    V s[H + 1], d[H + 1];
+    static_for<1, H + 1>([&](auto t) {
+      s[t] = cadd(x[t], x[N - t]);
+      d[t] = csub(x[t], x[N - t]);
+    });
+    V out[N];
+    V o0 = x[0];
+    static_for<1, H + 1>([&](auto t) { o0 = cadd(o0, s[t]); });
+    out[0] = o0;
+    static_for<1, H + 1>([&](auto q) {
+      V re = x[0];
+      R ir = 0, ii = 0;
+      static_for<1, H + 1>([&](auto t) {
+        constexpr long tq = static_cast<long>(SPO_CV(t)) * SPO_CV(q) % N;
+        constexpr R c = static_cast<R>(Root<tq, N, S>::re);
+        constexpr R sn = static_cast<R>(Root<tq, N, S>::im);
+        re = cmake<V>(re.x + c * s[t].x, re.y + c * s[t].y);
+        ir += sn * d[t].x;
+        ii += sn * d[t].y;
+      });
+      const V rot = cmake<V>(-ii, ir);  // i * sum Im(w) d
+      out[q] = cadd(re, rot);
+      out[N - q] = csub(re, rot);
+    });
+    static_for<0, N>([&](auto t) { x[t] = out[t]; });
+  } else {
+    constexpr int P = first_factor(N);
+    constexpr int Q = N / P;
+    V y[N];
+    static_for<0, P>([&](auto p) {
+      V sub[Q];
+      static_for<0, Q>([&](auto q) { sub[q] = x[p + P * q]; });
+      rdft<Q, S>(sub);
+      static_for<0, Q>([&](auto k1) {
+        y[p * Q + k1] = twiddle_mul<V, static_cast<long>(SPO_CV(p)) * SPO_CV(k1), N, S>(sub[k1]);
+      });
+    });
+    static_for<0, Q>([&](auto k1) {
+      V t[P];
+      static_for<0, P>([&](auto p) { t[p] = y[p * Q + k1]; });
+      rdft<P, S>(t);
+      static_for<0, P>([&](auto k2) { x[k1 + Q * k2] = t[k2]; });
+    });
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Two-level axis pass: FFT along an axis of length N = N1 N2 of an array (outer, N, inner), for TB
+// consecutive inner elements per block; forward, times a factor f[k], inverse (the kinetic step
+// exp(-i T dt) of one coordinate, with the FFT scales folded into f).
+//   forward:  thread (b, n2) loads x[n2 + N2 n1] (n1 < N1) from global memory, DFT_N1 in registers,
+//             times w_N^(n2 k1), into shared memory Y[n2][k1][b]; thread (b, k1) loads Y[.][k1][b],
+//             DFT_N2: X[k1 + N1 k2].
+//   factor:   X[k] *= f[k] in the same registers.
+//   inverse:  the same two levels backwards (IDFT_N2, conjugate twiddle, shared memory, IDFT_N1),
+//             stored straight to global memory.
+// One shared-memory round trip per direction; each thread reads and writes only its own Y entries
+// between the two halves, so one buffer serves both.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+struct Axis2Args {
+  Vec<T>* data;
+  long long inner;
+  const Vec<T>* factor;  // N values, by k
+  const Vec<T>* tw;      // N values: exp(-2 pi i j / N)
+};
+
+// Dynamic shared memory: (N TB + 2 N) values (axis2_smem).
+template <typename T, int N1, int N2, int TB>
+__global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2_kernel(Axis2Args<T> a) {
+  using V = Vec<T>;
+  constexpr int N = N1 * N2;
+  constexpr int NS = N1 > N2 ? N1 : N2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* Y = reinterpret_cast<V*>(smem_raw);
+  V* f = Y + N * TB;
+  V* tw = f + N;
+  const int b = threadIdx.x % TB;
+  const int s = threadIdx.x / TB;
+  const long long i0 = static_cast<long long>(blockIdx.x) * TB;
+  const long long base = static_cast<long long>(blockIdx.y) * N * a.inner + i0 + b;
+  const bool lane_ok = i0 + b < a.inner;
+  for (int k = threadIdx.x; k < N; k += TB * NS) {
+    f[k] = a.factor[k];
+    tw[k] = a.tw[k];
+  }
+  __syncthreads();
+  // forward, level 1
+  if (s < N2) {
+    const int n2 = s;
+    V x[N1];
+    static_for<0, N1>([&](auto n1) {
+      x[n1] = lane_ok ? a.data[base + static_cast<long long>(n2 + N2 * n1) * a.inner] : cmake<V>(0, 0);
+    });
+    rdft<N1, -1>(x);
+    static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : cmul(x[k1], tw[n2 * k1]); });
+  }
+  __syncthreads();
+  // forward level 2, factor, inverse level 2
+  if (s < N1) {
+    const int k1 = s;
+    V y[N2];
+    static_for<0, N2>([&](auto n2) { y[n2] = Y[(n2 * N1 + k1) * TB + b]; });
+    rdft<N2, -1>(y);
+    static_for<0, N2>([&](auto k2) { y[k2] = cmul(f[k1 + N1 * k2], y[k2]); });
+    rdft<N2, +1>(y);
+    static_for<0, N2>([&](auto n2) { Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : cmul(y[n2], cconj(tw[n2 * k1])); });
+  }
+  __syncthreads();
+  // inverse level 1, store
+  if (s < N2 && lane_ok) {
+    const int n2 = s;
+    V x[N1];
+    static_for<0, N1>([&](auto k1) { x[k1] = Y[(n2 * N1 + k1) * TB + b]; });
+    rdft<N1, +1>(x);
+    static_for<0, N1>([&](auto n1) { a.data[base + static_cast<long long>(n2 + N2 * n1) * a.inner] = x[n1]; });
+  }
+}
+
+}  // namespace spo
+
+namespace spo {
+
+// ---------------------------------------------------------------------------------------------
+// xy pass with register DFTs: exp(-i T_xy dt) at one (Z, r) point for TB rotational states
+// (src/propagation/kinetic_operators.cpp:134-172), the gas-phase potential step fused for
+// Z >= zasymp (potential_operator.cpp:104-112).
+//   y forward:  thread (b, ix) loads psi[ix, 0..NY) (times the momentum shift), DFT_NY, -> S[ix][ky][b]
+//   x:          thread (b, ky) loads S[0..NX)[ky][b], DFT_NX, times the factor, IDFT_NX, back in place
+//   y inverse:  thread (b, ix) loads S[ix][0..NY)[b], IDFT_NY, shift back, (gas W), stores psi.
+// ---------------------------------------------------------------------------------------------
+template <typename T, int NX, int NY, int TB>
+__global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2_kernel(XyArgs<T> a) {
+  using V = Vec<T>;
+  constexpr int NXY = NX * NY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* S = reinterpret_cast<V*>(smem_raw);  // NXY * TB
+  V* f = S + NXY * TB;                     // NXY
+  const int b = threadIdx.x % TB;
+  const int s = threadIdx.x / TB;
+  const long long izr = blockIdx.y;
+  const int irot = blockIdx.x * TB + b;
+  const bool lane_ok = irot < a.n_rot;
+  const long long col0 = izr * NXY;
+  for (int k = threadIdx.x; k < NXY; k += blockDim.x) f[k] = a.factor[k];
+  if (s < NX) {
+    const int ix = s;
+    V x[NY];
+    static_for<0, NY>([&](auto iy) {
+      V v = cmake<V>(0, 0);
+      if (lane_ok) {
+        v = a.psi[(col0 + ix * NY + iy) * a.n_rot + irot];
+        if (a.shift_f) v = cmul(v, a.shift_f[ix * NY + iy]);
+      }
+      x[iy] = v;
+    });
+    rdft<NY, -1>(x);
+    static_for<0, NY>([&](auto ky) { S[(ix * NY + ky) * TB + b] = x[ky]; });
+  }
+  __syncthreads();
+  if (s < NY) {
+    const int ky = s;
+    V x[NX];
+    static_for<0, NX>([&](auto ix) { x[ix] = S[(ix * NY + ky) * TB + b]; });
+    rdft<NX, -1>(x);
+    static_for<0, NX>([&](auto kx) { x[kx] = cmul(f[kx * NY + ky], x[kx]); });
+    rdft<NX, +1>(x);
+    static_for<0, NX>([&](auto ix) { S[(ix * NY + ky) * TB + b] = x[ix]; });
+  }
+  __syncthreads();
+  if (s < NX && lane_ok) {
+    const int ix = s;
+    V x[NY];
+    static_for<0, NY>([&](auto ky) { x[ky] = S[(ix * NY + ky) * TB + b]; });
+    rdft<NY, +1>(x);
+    const bool gas = a.apply_gas && izr >= a.izr_gas_first;
+    const int ir = static_cast<int>(izr % a.nr);
+    V g = cmake<V>(1, 0);
+    if (gas) g = cscale(a.gas_step[ir * a.n_rot + irot], a.opt_z[izr / a.nr]);
+    static_for<0, NY>([&](auto iy) {
+      V v = x[iy];
+      if (a.shift_b) v = cmul(v, a.shift_b[ix * NY + iy]);
+      if (gas) v = cmul(g, v);
+      a.psi[(col0 + ix * NY + iy) * a.n_rot + irot] = v;
+    });
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Potential step of the interaction region with register phi transforms: one (Z, r) point per
+// block, CB (x, y) columns per chunk, one thread per (column, theta) line.
+//   load:     the CB columns (absorption, rot(dt/2), the specular wave into the initial channel)
+//             into shared memory F[c][irot];
+//   forward:  thread (c, theta) forms its line's phi slots by the theta contraction of every mJ block
+//             straight into registers (slot p of mJ = p or p - NPHI), DFT_NPHI (sign +1);
+//   exp(iA):  times exp(i A) of the column's representative at the mapped phi;
+//   back:     IDFT_NPHI (sign -1), the line into shared memory D[c][theta][p];
+//   transpose sums: thread j takes rotational states irot = j, j + blockDim.x, ... and sums over
+//             theta for all CB columns at once (one matrix element reused CB times), times rot(dt/2);
+//   projection: the initial channel of every column of the point is kept and projected onto the
+//             specular grid at the end in a fixed order (src/propagation/potential_operator.cpp:129-135).
+// The matrix is read as legendre (block, theta, J) from shared memory by the transposed sums and as
+// legendre_t (block, J, theta) through the read-only cache by the forward sums.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+struct Pot2Args {
+  PotArgs<T> p;
+  const T* legendre_t;  // (block, J, theta)
+  int cb;
+  int identity_maps;    // no symmetry: representative = ixy and phi map = identity
+};
+
+template <typename T, int NPHI, int CB>
+__global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
+  using V = Vec<T>;
+  const PotArgs<T>& a = args.p;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n_rot = a.n_rot, nt = a.n_theta;
+  constexpr int LD = NPHI + 1;
+  V* F = reinterpret_cast<V*>(smem_raw);  // CB * n_rot
+  V* D = F + CB * n_rot;                  // CB * nt * LD
+  V* i0buf = D + CB * nt * LD;            // n_xy
+  V* red = i0buf + a.n_xy;                // 32
+  T* leg = reinterpret_cast<T*>(red + 32);  // nt * n_rot, (block, theta, J)
+  const int izr = blockIdx.x;
+  const int ir = izr % a.nr;
+  const int iz = izr / a.nr;
+  const int i0 = a.initial_channel;
+  const int mj_max = a.mj_max;
+  for (int k = threadIdx.x; k < nt * n_rot; k += blockDim.x) leg[k] = a.legendre[k];
+  const T oz = a.opt_z[iz];
+  const V incoming = a.chi[ir + a.nr * iz];
+  const V rot_i0 = a.rot_half[ir * n_rot + i0];
+  const long long col_base = static_cast<long long>(izr) * a.n_xy;
+  const long long e_base = static_cast<long long>(izr) * a.n_rep * nt * NPHI;
+  const int line_c = threadIdx.x / nt;  // this thread's line: column line_c, theta line_t
+  const int line_t = threadIdx.x % nt;
+  __syncthreads();
+
+  for (int c0 = 0; c0 < a.n_xy; c0 += CB) {
+    const int ncol = min(CB, a.n_xy - c0);
+    for (int e = threadIdx.x; e < ncol * n_rot; e += blockDim.x) {
+      const int c = e / n_rot, irot = e - c * n_rot;
+      const int ixy = c0 + c;
+      V v = a.psi[(col_base + ixy) * n_rot + irot];
+      v = cscale(cmul(a.before[ir * n_rot + irot], v), oz);
+      if (irot == i0) v = cadd(v, cmul(rot_i0, cmul(a.sp2sc[ixy], incoming)));
+      F[c * n_rot + irot] = v;
+    }
+    __syncthreads();
+    if (line_c < ncol) {
+      const int c = line_c, t = line_t;
+      const int ixy = c0 + c;
+      const V* f = F + c * n_rot;
+      V x[NPHI];
+      static_for<0, NPHI>([&](auto p) {
+        constexpr int P = SPO_CV(p);
+        const int m = P <= mj_max ? P : (P >= NPHI - mj_max ? P - NPHI : 1 << 20);
+        V s = cmake<V>(0, 0);
+        if (m != (1 << 20)) {
+          const int blk = mj_max + m;
+          const int nj = a.block_size[blk];
+          const int first = a.block_first[blk];
+          const T* mt = args.legendre_t + a.block_offset[blk] + t;  // (J, theta) within the block
+          for (int j = 0; j < nj; ++j) {
+            const T w = __ldg(mt + j * nt);
+            const V fv = f[first + j];
+            s = cmake<V>(s.x + w * fv.x, s.y + w * fv.y);
+          }
+        }
+        x[P] = s;
+      });
+      rdft<NPHI, +1>(x);
+      if (args.identity_maps) {
+        const V* e = a.expia + e_base + (static_cast<long long>(ixy) * nt + t) * NPHI;
+        static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + p), x[p]); });
+      } else {
+        const V* e = a.expia + e_base + (static_cast<long long>(a.rep_of[ixy]) * nt + t) * NPHI;
+        const int* map = a.phi_map + ixy * NPHI;
+        static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + __ldg(map + p)), x[p]); });
+      }
+      rdft<NPHI, -1>(x);
+      static_for<0, NPHI>([&](auto p) { D[(c * nt + t) * LD + p] = x[p]; });
+    }
+    __syncthreads();
+    for (int irot = threadIdx.x; irot < n_rot; irot += blockDim.x) {
+      const int blk = a.irot_block[irot];
+      const int nj = a.block_size[blk];
+      const int jj = irot - a.block_first[blk];
+      const int slot = a.block_slot[blk];
+      const T* col = leg + a.block_offset[blk] + jj;
+      V acc[CB];
+#pragma unroll
+      for (int c = 0; c < CB; ++c) acc[c] = cmake<V>(0, 0);
+      for (int t = 0; t < nt; ++t) {
+        const T w = col[t * nj];
+        const V* d = D + t * LD + slot;
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+          const V dv = d[c * nt * LD];
+          acc[c] = cmake<V>(acc[c].x + w * dv.x, acc[c].y + w * dv.y);
+        }
+      }
+      const V rh = a.rot_half[ir * n_rot + irot];
+#pragma unroll
+      for (int c = 0; c < CB; ++c) {
+        if (c < ncol) {
+          const V s = cmul(rh, acc[c]);
+          if (irot == i0) i0buf[c0 + c] = s;
+          else a.psi[(col_base + c0 + c) * n_rot + irot] = s;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 32) {
+    V s = cmake<V>(0, 0);
+    for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += 32) s = cadd(s, cmul(a.sc2sp[ixy], i0buf[ixy]));
+    red[threadIdx.x] = s;
+    __syncwarp();
+    if (threadIdx.x == 0) {
+      V p = cmake<V>(0, 0);
+      for (int k = 0; k < 32; ++k) p = cadd(p, red[k]);
+      red[0] = p;
+      a.chi[ir + a.nr * iz] = p;
+    }
+  }
+  __syncthreads();
+  const V proj = red[0];
+  for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += blockDim.x)
+    a.psi[(col_base + ixy) * n_rot + i0] = csub(i0buf[ixy], cmul(a.sp2sc[ixy], proj));
+}
+
+}  // namespace spo

@@ -146,6 +146,43 @@ class B200Backend:
         self._check(self._lib.spo_site_column(self._h, int(ixy), capi.dptr(out)))
         return out
 
+    # ------------------------------------------------------------------ asymptotic analysis (FP64)
+    def analysis_setup(self, analysis: dict, phi_vj: np.ndarray, energies_hartree: np.ndarray) -> None:
+        """Balint-Kurti analysis data (AnalysisBasis, GasPhase, AnalysisEnergies of the reference):
+        `analysis` holds n_v, n_rotation, n_diffraction, rotation_index, rotation_j, channel_ix,
+        channel_iy, j_max_gas, initial_state, j_in, iz_analysis, dr, xy_scale, analysis_time_step."""
+        a = analysis
+        keep = {k: _i(a[k]) for k in ("rotation_index", "rotation_j", "channel_ix", "channel_iy")}
+        keep["phi"] = _f(phi_vj)
+        keep["e"] = _f(energies_hartree)
+        d = capi.SpoAnalysisDesc()
+        for k in ("n_v", "n_rotation", "n_diffraction", "j_max_gas", "initial_state", "j_in", "iz_analysis"):
+            setattr(d, k, int(a[k]))
+        for k in ("dr", "xy_scale", "analysis_time_step"):
+            setattr(d, k, float(a[k]))
+        for k in ("rotation_index", "rotation_j", "channel_ix", "channel_iy"):
+            setattr(d, k, capi.iptr(keep[k]))
+        d.phi_vj = capi.dptr(keep["phi"])
+        d.n_energies = int(keep["e"].size)
+        d.energies_hartree = capi.dptr(keep["e"])
+        self._check(self._lib.spo_analysis_setup(self._h, ctypes.byref(d)))
+        self._n_bk = int(a["n_v"]) * int(a["n_rotation"]) * int(a["n_diffraction"])
+        self._n_e = int(keep["e"].size)
+
+    def bk_coefficients(self, time: float = 0.0, surface_fixed: bool = False, surface_index: int = 0,
+                        accumulate: bool = False) -> np.ndarray:
+        """BK coefficients (n_v, n_states) of the current wave packet (BalintKurtiAnalyzer::coefficients)."""
+        out = np.empty(self._n_bk, dtype=np.complex128)
+        self._check(self._lib.spo_bk_coefficients(self._h, float(time), 1 if surface_fixed else 0,
+                                                  int(surface_index), 1 if accumulate else 0, capi.dptr(out)))
+        return out
+
+    def s_matrix_sums(self) -> np.ndarray:
+        """(n_energies, n_v * n_states): sum_t c(t) exp(i E t) dt_analysis (SMatrixAccumulator::add)."""
+        out = np.empty(self._n_e * self._n_bk, dtype=np.complex128)
+        self._check(self._lib.spo_s_matrix_sums(self._h, capi.dptr(out)))
+        return out.reshape(self._n_e, self._n_bk)
+
     # ------------------------------------------------------------------ diagnostics
     def apply_stage(self, stage: int, half: bool = False) -> None:
         self._check(self._lib.spo_apply_stage(self._h, int(stage), 1 if half else 0))

@@ -27,7 +27,7 @@ EXPORTS = [
     "spo_upload_state", "spo_download_state", "spo_get_specular", "spo_get_z_plane",
     "spo_block_densities", "spo_site_column", "spo_apply_stage", "spo_set_stream", "spo_profile",
     "spo_profile_count", "spo_profile_entry", "spo_device_bytes", "spo_last_launch_count",
-    "spo_block_densities_noalloc",
+    "spo_block_densities_noalloc", "spo_analysis_setup", "spo_bk_coefficients", "spo_s_matrix_sums",
 ]
 NOALLOC_MAX_BLOCKS = 65536
 
@@ -56,6 +56,18 @@ class SpoDesc(ctypes.Structure):
         ("n_rep", ctypes.c_int), ("n_ops", ctypes.c_int), ("potential", _dp),
         ("representative_of", _ip), ("operation_of", _ip), ("phi_index", _ip),
         ("chi_initial", _dp), ("precision", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+class SpoAnalysisDesc(ctypes.Structure):
+    """struct spo_analysis_desc of include/spo_b200.h."""
+
+    _fields_ = [
+        ("n_v", ctypes.c_int), ("n_rotation", ctypes.c_int), ("n_diffraction", ctypes.c_int),
+        ("rotation_index", _ip), ("rotation_j", _ip), ("channel_ix", _ip), ("channel_iy", _ip),
+        ("j_max_gas", ctypes.c_int), ("phi_vj", _dp), ("initial_state", ctypes.c_int), ("j_in", ctypes.c_int),
+        ("iz_analysis", ctypes.c_int), ("dr", ctypes.c_double), ("xy_scale", ctypes.c_double),
+        ("n_energies", ctypes.c_int), ("energies_hartree", _dp), ("analysis_time_step", ctypes.c_double),
     ]
 
 
@@ -91,6 +103,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.spo_profile_count.argtypes = [h, _ip]
     lib.spo_profile_entry.argtypes = [h, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp, _ip, _dp]
     lib.spo_device_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.spo_analysis_setup.argtypes = [h, ctypes.POINTER(SpoAnalysisDesc)]
+    lib.spo_bk_coefficients.argtypes = [h, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
+    lib.spo_s_matrix_sums.argtypes = [h, _dp]
     lib.spo_block_densities_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong,
                                                 _dp, ctypes.c_void_p]
     lib.spo_last_launch_count.argtypes = [h, _ip]

@@ -143,6 +143,45 @@ int spo_block_densities(spo_handle* h, double* out);
  * complex). Replaces PropagationBackend::site_column (propagation_backend.hpp:58). */
 int spo_site_column(spo_handle* h, int ixy, double* out);
 
+/* ---------------------------------------------------------------------------------------------
+ * Asymptotic analysis on the device, in FP64 whatever the precision form: the Balint-Kurti
+ * projection at the analysis line (BalintKurtiAnalyzer::coefficients, src/analysis/balint_kurti.cpp:
+ * 39-84) and the on-the-fly S-matrix sums (SMatrixAccumulator::add, src/analysis/s_matrix.cpp:49-56).
+ * The data are those of AnalysisBasis, GasPhase and AnalysisEnergies of the reference.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct spo_analysis_desc {
+  int n_v;                    /* vibrational levels analysed (AnalysisBasis::n_v) */
+  int n_rotation;             /* analysed rotational states (AnalysisBasis::n_rotation) */
+  int n_diffraction;          /* diffraction channels (AnalysisBasis::n_diffraction) */
+  const int* rotation_index;  /* n_rotation: index of each analysed state in the propagation basis */
+  const int* rotation_j;      /* n_rotation: its J */
+  const int* channel_ix;      /* n_diffraction: (x, y) FFT slot of each diffraction channel */
+  const int* channel_iy;
+  int j_max_gas;              /* phi_vj holds j = 0 .. j_max_gas */
+  const double* phi_vj;       /* (ir, j, v): the gas-phase vibrational functions phi_vj(r) */
+  int initial_state;          /* is of (JIn, MJIn, n = m = 0) */
+  int j_in;
+  int iz_analysis;            /* Z index of the analysis line on the scattering grid */
+  double dr;                  /* r grid step */
+  double xy_scale;            /* sqrt(dx dy sin(skew) / (nx ny)) */
+  int n_energies;
+  const double* energies_hartree;  /* the analysis energies (total, hartree) */
+  double analysis_time_step;       /* steps_per_analysis * dt */
+} spo_analysis_desc;
+
+/* Uploads the analysis data; the S-matrix sums start at zero. */
+int spo_analysis_setup(spo_handle* h, const spo_analysis_desc* d);
+
+/* BK coefficients of the current wave packet, (is, v) with is = irotana * n_diffraction + idif
+ * (n_rotation * n_diffraction * n_v complex) into bk_out (may be NULL). With surface_fixed != 0 the
+ * initial state's coefficient comes from the specular wave at surface_index (the fixed specular
+ * analysis line). With accumulate != 0 they are also added to the S-matrix sums at `time`. */
+int spo_bk_coefficients(spo_handle* h, double time, int surface_fixed, int surface_index, int accumulate,
+                        double* bk_out);
+
+/* The S-matrix sums, (is, v, ien): n_rotation * n_diffraction * n_v * n_energies complex. */
+int spo_s_matrix_sums(spo_handle* h, double* out);
+
 /* Operators of one sub-step, for stage-by-stage checks (the reference tests its operators one by one:
  * tests/test_propagation.cpp, test_cuda_backend.cpp:161-278). */
 enum spo_stage {

@@ -350,6 +350,7 @@ int run_case(const Options& o) {
   std::vector<spodvr::BkCoefficients> records;
   std::vector<cplx> chis;
   std::vector<int> surface_index;
+  std::vector<double> times;
   const spodvr::InputParameters& p = config.input;
   const int n_per_analysis = config.derived.steps_per_analysis;
   const auto t0 = std::chrono::steady_clock::now();
@@ -359,6 +360,7 @@ int run_case(const Options& o) {
     records.push_back(bk.coefficients(backend->z_plane(s.grids->iz_analysis), backend->specular(), surface));
     const double time = p.t_end + ((a + 1) * n_per_analysis - p.n_steps) * p.time_step;
     s_matrix.add(records.back(), time);
+    times.push_back(time);
     const auto& chi = backend->specular().values;
     chis.insert(chis.end(), chi.begin(), chi.end());
     surface_index.push_back(surface.fixed() ? surface.index() : -1 - surface.index());
@@ -367,6 +369,7 @@ int run_case(const Options& o) {
   write_vec(o.out / "chi_steps.c128", chis);
   write_bk(o.out / "bk_steps.c128", records);
   write_vec(o.out / "surface_index.i32", surface_index);
+  write_vec(o.out / "analysis_times.f64", times);
   const spodvr::WavePacket& psi = backend->wave_packet_on_host();
   if (o.dump_psi) write_vec(o.out / "psi_final.c128", std::vector<cplx>(psi.scattering.values.begin(), psi.scattering.values.end()));
   write_vec(o.out / "block_densities.f64", backend->block_densities());

@@ -319,3 +319,10 @@ def bk_coefficients(z_plane: np.ndarray, chi: np.ndarray, case: Case, surface_fi
         for v in range(n_v):
             bk[v, a["initial_state"]] = np.sum(chi[surface_index, :] * phi[v, a["j_in"]]) * case.dr
     return bk
+
+
+def s_matrix_sums(bk_steps: np.ndarray, times: np.ndarray, energies_hartree: np.ndarray, dt_analysis: float):
+    """SMatrixAccumulator::add over analysis steps (s_matrix.cpp:49-56): sums[ien, k] = sum_t bk_t[k]
+    exp(i E_ien t) dt_analysis. bk_steps: (steps, n) with k = is + n_states v."""
+    phase = np.exp(1j * np.outer(energies_hartree, times))          # (ien, t)
+    return (phase @ bk_steps) * dt_analysis                          # (ien, k)
