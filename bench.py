@@ -158,9 +158,10 @@ def measure(case, precision, steps, warmup, device, world):
     e2e_ms = e0.elapsed_time(e1)
     h2d = (psi0.nbytes + chi0.nbytes) / steps
     d2h = chi.nbytes + plane.nbytes
+    kernels = be.describe()
     be.close()
     return {"ms": ms, "launches": launches, "records": records, "clocks": clock, "e2e_ms": e2e_ms,
-            "h2d": h2d, "d2h": d2h}
+            "h2d": h2d, "d2h": d2h, "kernels": kernels}
 
 
 def reduce_max(x, world, device):
@@ -288,7 +289,8 @@ def main():
                        "points": int(points), "step": "one analysis step = 5 time steps",
                        "time_steps_per_step": case.steps_per_analysis,
                        "l2": "inputs larger than L2 (psi 3.2 GB mixed / 6.4 GB FP64, table 2.6 / 5.3 GB)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}",
+                       "kernels_mixed": m["kernels"], "kernels_fp64": res["fp64"]["kernels"]},
             "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms"] / args.steps,
                      "e2e": out["fp64"]["e2e"]},
             "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],

@@ -27,6 +27,7 @@
 #include "../../include/spo_b200.h"
 #include "spo_kernels.cuh"
 #include "spo_regfft.cuh"
+#include "spo_pot4.cuh"
 
 namespace {
 
@@ -137,41 +138,64 @@ struct Sizes {
 // Launchers of the register-DFT kernels for the sizes they are instantiated for. Each returns
 // false for other sizes; the caller then uses the general shared-memory Stockham kernels.
 // ---------------------------------------------------------------------------------------------
-template <typename T, int N1, int N2>
-bool launch_axis2_n(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
+// Sets a kernel's dynamic shared-memory limit once per device (the attribute is per device context).
+template <typename K>
+void allow_smem(K kernel, std::size_t bytes, unsigned long long& done_mask, const char* what) {
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 64 && (done_mask >> dev & 1ull)) return;
+  check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)), what);
+  if (dev < 64) done_mask |= 1ull << dev;
+}
+
+// The device's largest dynamic shared memory per block (opt-in).
+std::size_t smem_optin_bytes() {
+  int dev = 0, optin = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "smem attribute");
+  return static_cast<std::size_t>(optin);
+}
+
+template <typename T, int N1, int N2, int TB>
+bool launch_axis2_tb(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
   constexpr int NS = N1 > N2 ? N1 : N2;
-  constexpr int TB = NS <= 8 ? 32 : 16;
   constexpr int N = N1 * N2;
   const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(N) * TB + 2 * N);
-  static bool configured = false;
-  if (!configured) {
-    check_cuda(cudaFuncSetAttribute(spo::axis2_kernel<T, N1, N2, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)),
-               "axis2 smem");
-    configured = true;
-  }
+  static unsigned long long configured = 0;
+  allow_smem(spo::axis2_kernel<T, N1, N2, TB>, smem, configured, "axis2 smem");
   const dim3 grid(static_cast<unsigned>((a.inner + TB - 1) / TB), static_cast<unsigned>(outer));
   spo::axis2_kernel<T, N1, N2, TB><<<grid, TB * NS, smem, stream>>>(a);
   return true;
 }
 
+// Tile width (batch lanes per block): 32 lanes when a line has at most 8 sub-rows; for 16 sub-rows
+// 16 lanes (256 threads) or, when the autotuner chose it (wide), 32 lanes (512 threads).
+template <typename T, int N1, int N2>
+bool launch_axis2_n(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
+  constexpr int NS = N1 > N2 ? N1 : N2;
+  if constexpr (NS <= 8) return launch_axis2_tb<T, N1, N2, 32>(a, outer, stream);
+  else if (a.wide) return launch_axis2_tb<T, N1, N2, 32>(a, outer, stream);
+  else return launch_axis2_tb<T, N1, N2, 16>(a, outer, stream);
+}
+
 template <typename T>
 bool launch_axis2(int n, const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
   switch (n) {
-    case 24: return launch_axis2_n<T, 6, 4>(a, outer, stream);
-    case 32: return launch_axis2_n<T, 8, 4>(a, outer, stream);
-    case 40: return launch_axis2_n<T, 8, 5>(a, outer, stream);
-    case 48: return launch_axis2_n<T, 8, 6>(a, outer, stream);
-    case 56: return launch_axis2_n<T, 8, 7>(a, outer, stream);
+    // N = N1 N2 with N2 >= N1: the first level, which streams the tile in from HBM, uses every thread.
+    case 24: return launch_axis2_n<T, 4, 6>(a, outer, stream);
+    case 32: return launch_axis2_n<T, 4, 8>(a, outer, stream);
+    case 40: return launch_axis2_n<T, 5, 8>(a, outer, stream);
+    case 48: return launch_axis2_n<T, 6, 8>(a, outer, stream);
+    case 56: return launch_axis2_n<T, 7, 8>(a, outer, stream);
     case 64: return launch_axis2_n<T, 8, 8>(a, outer, stream);
-    case 80: return launch_axis2_n<T, 10, 8>(a, outer, stream);
-    case 96: return launch_axis2_n<T, 12, 8>(a, outer, stream);
-    case 112: return launch_axis2_n<T, 16, 7>(a, outer, stream);
-    case 128: return launch_axis2_n<T, 16, 8>(a, outer, stream);
-    case 160: return launch_axis2_n<T, 16, 10>(a, outer, stream);
-    case 176: return launch_axis2_n<T, 16, 11>(a, outer, stream);
-    case 192: return launch_axis2_n<T, 16, 12>(a, outer, stream);
-    case 224: return launch_axis2_n<T, 16, 14>(a, outer, stream);
+    case 80: return launch_axis2_n<T, 8, 10>(a, outer, stream);
+    case 96: return launch_axis2_n<T, 8, 12>(a, outer, stream);
+    case 112: return launch_axis2_n<T, 7, 16>(a, outer, stream);
+    case 128: return launch_axis2_n<T, 8, 16>(a, outer, stream);
+    case 160: return launch_axis2_n<T, 10, 16>(a, outer, stream);
+    case 176: return launch_axis2_n<T, 11, 16>(a, outer, stream);
+    case 192: return launch_axis2_n<T, 12, 16>(a, outer, stream);
+    case 224: return launch_axis2_n<T, 14, 16>(a, outer, stream);
     case 256: return launch_axis2_n<T, 16, 16>(a, outer, stream);
     default: return false;
   }
@@ -184,20 +208,24 @@ bool axis2_supported(int n) {
   }
 }
 
+bool xy2_supported(int n) { return n == 2 || n == 4 || n == 6 || n == 8 || n == 12 || n == 16; }
+
+template <typename T, int NX, int NY, int TB>
+void launch_xy2_tb(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream) {
+  constexpr int NS = NX > NY ? NX : NY;
+  const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(NX * NY) * TB + NX * NY);
+  static unsigned long long configured = 0;
+  allow_smem(spo::xy2_kernel<T, NX, NY, TB>, smem, configured, "xy2 smem");
+  const dim3 grid(static_cast<unsigned>((a.n_rot + TB - 1) / TB), static_cast<unsigned>(n_zr));
+  spo::xy2_kernel<T, NX, NY, TB><<<grid, TB * NS, smem, stream>>>(a);
+}
+
 template <typename T, int NX, int NY>
 void launch_xy2_n(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream) {
   constexpr int NS = NX > NY ? NX : NY;
-  constexpr int TB = NS <= 8 ? 32 : 16;
-  const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(NX * NY) * TB + NX * NY);
-  static bool configured = false;
-  if (!configured) {
-    check_cuda(cudaFuncSetAttribute(spo::xy2_kernel<T, NX, NY, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)),
-               "xy2 smem");
-    configured = true;
-  }
-  const dim3 grid(static_cast<unsigned>((a.n_rot + TB - 1) / TB), static_cast<unsigned>(n_zr));
-  spo::xy2_kernel<T, NX, NY, TB><<<grid, TB * NS, smem, stream>>>(a);
+  if constexpr (NS <= 8) launch_xy2_tb<T, NX, NY, 32>(a, n_zr, stream);
+  else if (a.wide) launch_xy2_tb<T, NX, NY, 32>(a, n_zr, stream);
+  else launch_xy2_tb<T, NX, NY, 16>(a, n_zr, stream);
 }
 
 template <typename T>
@@ -224,16 +252,10 @@ std::size_t pot2_smem(int cb, int n_rot, int nt, int nphi, long long n_xy) {
 
 template <typename T, int NPHI, int CB>
 void launch_pot2_n(const spo::Pot2Args<T>& a, unsigned blocks, std::size_t smem, cudaStream_t stream) {
-  static bool configured = false;
-  if (!configured) {
-    int dev = 0, optin = 0;
-    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-    check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "smem attribute");
-    check_cuda(cudaFuncSetAttribute(spo::potential2_kernel<T, NPHI, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    optin),
-               "potential2 smem");
-    configured = true;
-  }
+  // The shared memory depends on the case's sizes, not only on the instantiation: allow the device's
+  // maximum, so that every case with this instantiation can launch.
+  static unsigned long long configured = 0;
+  allow_smem(spo::potential2_kernel<T, NPHI, CB>, smem_optin_bytes(), configured, "potential2 smem");
   spo::potential2_kernel<T, NPHI, CB><<<blocks, 128, smem, stream>>>(a);
 }
 
@@ -261,6 +283,57 @@ void launch_pot2(int nphi, const spo::Pot2Args<T>& a, unsigned blocks, std::size
     default: break;
   }
 }
+// Shared memory of potential3_kernel<T, NPHI, CB>: F (slot-major, jp values per slot) and D share it.
+template <typename T>
+std::size_t pot3_smem(int cb, int jp, int nt, int nphi) {
+  return sizeof(spo::Vec<T>) * std::max(static_cast<std::size_t>(cb) * (static_cast<std::size_t>(nphi) * jp + 2),
+                                        static_cast<std::size_t>(cb) * nt * (nphi + 1));
+}
+
+template <typename T, int NPHI, int CB>
+void launch_pot3_n(const spo::Pot2Args<T>& a, dim3 grid, unsigned threads, std::size_t smem, cudaStream_t stream) {
+  static unsigned long long configured = 0;
+  allow_smem(spo::potential3_kernel<T, NPHI, CB>, smem_optin_bytes(), configured, "potential3 smem");
+  spo::potential3_kernel<T, NPHI, CB><<<grid, threads, smem, stream>>>(a);
+}
+
+template <typename T, int NPHI>
+void launch_pot3_phi(const spo::Pot2Args<T>& a, dim3 grid, unsigned threads, std::size_t smem, cudaStream_t stream) {
+  if (a.cb == 16) launch_pot3_n<T, NPHI, 16>(a, grid, threads, smem, stream);
+  else launch_pot3_n<T, NPHI, 8>(a, grid, threads, smem, stream);
+}
+
+template <typename T>
+void launch_pot3(int nphi, const spo::Pot2Args<T>& a, dim3 grid, unsigned threads, std::size_t smem,
+                 cudaStream_t stream) {
+  switch (nphi) {
+    case 6: launch_pot3_phi<T, 6>(a, grid, threads, smem, stream); break;
+    case 8: launch_pot3_phi<T, 8>(a, grid, threads, smem, stream); break;
+    case 10: launch_pot3_phi<T, 10>(a, grid, threads, smem, stream); break;
+    case 12: launch_pot3_phi<T, 12>(a, grid, threads, smem, stream); break;
+    case 16: launch_pot3_phi<T, 16>(a, grid, threads, smem, stream); break;
+    case 20: launch_pot3_phi<T, 20>(a, grid, threads, smem, stream); break;
+    case 24: launch_pot3_phi<T, 24>(a, grid, threads, smem, stream); break;
+    case 30: launch_pot3_phi<T, 30>(a, grid, threads, smem, stream); break;
+    case 32: launch_pot3_phi<T, 32>(a, grid, threads, smem, stream); break;
+    default: break;
+  }
+}
+
+// The potential4 instantiation for (nphi, ntheta), or null: ntheta 16, 8 and 4 with 8, 16 and 32 columns
+// per chunk, nphi 8, 16 and 32.
+template <typename T>
+using Pot4Kernel = void (*)(spo::Pot4Args<T>);
+template <typename T>
+Pot4Kernel<T> pot4_kernel_for(int nphi, int nt) {
+  if (nt == 16 && nphi == 32) return spo::potential4_kernel<T, 32, 16, 8>;
+  if (nt == 16 && nphi == 16) return spo::potential4_kernel<T, 16, 16, 8>;
+  if (nt == 8 && nphi == 16) return spo::potential4_kernel<T, 16, 8, 16>;
+  if (nt == 8 && nphi == 32) return spo::potential4_kernel<T, 32, 8, 16>;
+  if (nt == 4 && nphi == 8) return spo::potential4_kernel<T, 8, 4, 32>;
+  return nullptr;
+}
+
 bool pot2_phi_supported(int nphi) {
   switch (nphi) {
     case 6: case 8: case 10: case 12: case 16: case 20: case 24: case 30: case 32: return true;
@@ -346,6 +419,11 @@ class StepBase {
  public:
   virtual ~StepBase() = default;
   virtual void propagate_analysis_step() = 0;
+  // Queues one analysis step on the current stream without synchronising (graph capture).
+  virtual void enqueue_analysis_step() = 0;
+  virtual std::string describe() const = 0;
+  virtual void averages(const double* z, const double* zs, const double* r, double vol_scat, double vol_spec,
+                        int iz_analysis, int surface_index, double* out) = 0;
   virtual void upload(const double* psi, const double* chi) = 0;
   virtual void download(double* psi, double* chi) = 0;
   virtual void z_plane(int iz, double* out) = 0;
@@ -372,6 +450,12 @@ class Step final : public StepBase {
   }
 
   void propagate_analysis_step() override {
+    enqueue_analysis_step();
+    check_cuda(cudaStreamSynchronize(stream_), "propagate_analysis_step");
+    prof_.resolve();
+  }
+
+  void enqueue_analysis_step() override {
     launches_ = 0;
     const int n = s_.spa;
     for (int k = 0; k <= n; ++k) {
@@ -380,8 +464,31 @@ class Step final : public StepBase {
       sub_step(half, kinetic_only);
     }
     check_cuda(cudaGetLastError(), "propagate_analysis_step launch");
-    check_cuda(cudaStreamSynchronize(stream_), "propagate_analysis_step");
-    prof_.resolve();
+  }
+
+  std::string describe() const override {
+    auto axis_name = [&](int n, bool wide) {
+      if (!(use_v2_ && axis2_supported(n))) return std::string("axis_pass(general)");
+      return "axis2<" + std::to_string(n) + (wide ? ",wide>" : ",narrow>");
+    };
+    std::string out = std::string(sizeof(T) == 8 ? "fp64" : "mixed");
+    out += " z=" + axis_name(s_.nz, wide_z_);
+    out += " r=" + axis_name(s_.nr, wide_r_);
+    const bool xy2 = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx);
+    out += std::string(" xy=") + (xy2 ? "xy2<" + std::to_string(s_.nx) + (wide_xy_ ? ",wide>" : ",narrow>")
+                                      : std::string("xy_pass(general)"));
+    if (pot_kind_ == 4)
+      out += " potential=potential4<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
+             ",cb=" + std::to_string(128 / s_.nt) + ",blocks=" + std::to_string(pot4_blocks_) + ">";
+    else if (pot_kind_ == 3)
+      out += " potential=potential3<nphi=" + std::to_string(s_.nphi) + ",cb=" + std::to_string(pot3_cb_) +
+             ",chunks=" + std::to_string(pot3_chunks_) + ">";
+    else if (pot_kind_ == 2)
+      out += " potential=potential2<nphi=" + std::to_string(s_.nphi) + ",cb=" + std::to_string(pot2_cb_) + ">";
+    else
+      out += " potential=potential(general)";
+    out += " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
+    return out;
   }
 
   void upload(const double* psi, const double* chi) override {
@@ -410,6 +517,27 @@ class Step final : public StepBase {
     check_cuda(cudaMemcpyAsync(out, densities_, sizeof(double) * s_.n_zr(), cudaMemcpyDeviceToHost, stream_),
                "block_densities copy");
     check_cuda(cudaStreamSynchronize(stream_), "block_densities");
+  }
+
+  void averages(const double* z, const double* zs, const double* r, double vol_scat, double vol_spec, int iz_analysis,
+                int surface_index, double* out) override {
+    require(z && zs && r && out, "averages: null pointer");
+    require(iz_analysis >= -1 && iz_analysis < s_.nzs && surface_index < s_.nzs, "averages: index out of range");
+    // The grids and the four results pass through the staging buffer (>= 8M doubles).
+    double* g = reinterpret_cast<double*>(staging_);
+    const long long ng = static_cast<long long>(s_.nz) + s_.nzs + s_.nr;
+    require(ng + 4 <= 2 * staging_elems_, "averages: grids larger than the staging buffer");
+    check_cuda(cudaMemcpyAsync(g, z, sizeof(double) * s_.nz, cudaMemcpyHostToDevice, stream_), "averages grids");
+    check_cuda(cudaMemcpyAsync(g + s_.nz, zs, sizeof(double) * s_.nzs, cudaMemcpyHostToDevice, stream_), "averages grids");
+    check_cuda(cudaMemcpyAsync(g + s_.nz + s_.nzs, r, sizeof(double) * s_.nr, cudaMemcpyHostToDevice, stream_),
+               "averages grids");
+    spo::block_density_kernel<T><<<static_cast<unsigned>(s_.n_zr()), 256, 0, stream_>>>(
+        psi_, s_.n_xy() * s_.n_rot, densities_);
+    spo::averages_kernel<T><<<1, 256, 0, stream_>>>(densities_, chi_, g, s_.nz, s_.nr, s_.nzs, iz_analysis,
+                                                    surface_index, vol_scat, vol_spec, g + ng);
+    check_cuda(cudaGetLastError(), "averages launch");
+    check_cuda(cudaMemcpyAsync(out, g + ng, sizeof(double) * 4, cudaMemcpyDeviceToHost, stream_), "averages copy");
+    check_cuda(cudaStreamSynchronize(stream_), "averages");
   }
 
   void site_column(int ixy, double* out) override {
@@ -558,16 +686,16 @@ class Step final : public StepBase {
   // T_Z and T_r of the scattering wave.
   void kinetic_zr(bool half) {
     const double b = 2.0 * sizeof(V) * s_.n_psi();
-    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_);
-    axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_);
+    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, wide_z_);
+    axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, wide_r_);
   }
 
   // A kinetic axis pass over psi: the register-DFT kernel for its length when instantiated, else the
   // general Stockham kernel.
   void axis_psi(const char* name, double bytes, long long outer, const spo::FftPlan& plan, const V* tw,
-                long long inner, const V* factor) {
+                long long inner, const V* factor, bool wide) {
     if (use_v2_ && axis2_supported(plan.n)) {
-      spo::Axis2Args<T> a{psi_, inner, factor, tw};
+      spo::Axis2Args<T> a{psi_, inner, factor, tw, wide ? 1 : 0};
       prof_.begin(stream_);
       launch_axis2<T>(plan.n, a, outer, stream_);
       prof_.end(stream_, name, bytes);
@@ -597,6 +725,7 @@ class Step final : public StepBase {
     x.nr = s_.nr;
     x.opt_z = opt_z_;
     x.gas_step = gas_step_;
+    x.wide = wide_xy_ ? 1 : 0;
     const dim3 xg((s_.n_rot + xy_tb_ - 1) / xy_tb_, static_cast<unsigned>(s_.n_zr()));
     prof_.begin(stream_);
     if (!(use_v2_ && launch_xy2<T>(x, s_.n_zr(), stream_))) spo::xy_pass_kernel<T><<<xg, 256, xy_smem_, stream_>>>(x);
@@ -617,13 +746,89 @@ class Step final : public StepBase {
   void interaction() {
     if (s_.nzp == 0) return;
     prof_.begin(stream_);
-    if (use_v2_ && pot2_cb_ > 0)
-      launch_pot2<T>(s_.nphi, pot2_, static_cast<unsigned>(s_.nzp) * s_.nr, pot2_smem_, stream_);
+    const double bytes = sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia()));
+    const unsigned points = static_cast<unsigned>(s_.nzp) * s_.nr;
+    if (pot_kind_ == 3 || pot_kind_ == 4) {
+      if (pot_kind_ == 4) {
+        pot4_kernel_<<<pot4_blocks_, 128, pot4_smem_, stream_>>>(pot4_args_);
+      } else {
+        const dim3 grid(static_cast<unsigned>(pot3_chunks_), points);
+        launch_pot3<T>(s_.nphi, pot3_args_, grid, static_cast<unsigned>(pot3_cb_ * s_.nt), pot3_smem_, stream_);
+      }
+      prof_.end(stream_, "potential", bytes);
+      ++launches_;
+      prof_.begin(stream_);
+      spo::projection_finalize_kernel<T><<<points, 128, sizeof(V) * (s_.n_xy() + 1), stream_>>>(
+          psi_, chi_, s_.n_rot, static_cast<int>(s_.n_xy()), s_.i0, pot_.sc2sp, pot_.sp2sc);
+      prof_.end(stream_, "projection", 2.0 * sizeof(V) * points * s_.n_xy());
+      ++launches_;
+      return;
+    }
+    if (pot_kind_ == 2)
+      launch_pot2<T>(s_.nphi, pot2_, points, pot2_smem_, stream_);
     else
-      spo::potential_kernel<T><<<static_cast<unsigned>(s_.nzp) * s_.nr, 256, pot_smem_, stream_>>>(pot_);
-    prof_.end(stream_, "potential",
-              sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia())));
+      spo::potential_kernel<T><<<points, 256, pot_smem_, stream_>>>(pot_);
+    prof_.end(stream_, "potential", bytes);
     ++launches_;
+  }
+
+  // ------------------------------------------------------------------ tile choice
+  // Mean device milliseconds of `launch` over `reps` launches on the handle's stream, after one warm-up.
+  template <typename F>
+  float time_launches(F&& launch, int reps) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    launch();
+    check_cuda(cudaEventRecord(e0, stream_), "cudaEventRecord");
+    for (int i = 0; i < reps; ++i) launch();
+    check_cuda(cudaEventRecord(e1, stream_), "cudaEventRecord");
+    check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    float ms = 0.0f;
+    check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_cuda(cudaGetLastError(), "autotune launch");
+    return ms / reps;
+  }
+
+  // Chooses, per kinetic pass, between the narrow (16 lanes) and wide (32 lanes) tiles of the register
+  // kernels by timing both on the zero wave packet the handle starts with (a kinetic pass maps zero to
+  // zero, so the state is unchanged). Both tiles compute every line with the same operations in the
+  // same order: the choice changes the speed, never the result.
+  // SPO_B200_TILES=narrow|wide fixes the choice; SPO_B200_AUTOTUNE=0 keeps the narrow tiles.
+  void autotune() {
+    wide_z_ = wide_r_ = wide_xy_ = false;
+    tiles_source_ = "narrow";
+    if (!use_v2_) return;
+    if (const char* env = std::getenv("SPO_B200_TILES")) {
+      const std::string t(env);
+      require(t == "narrow" || t == "wide", "SPO_B200_TILES must be narrow or wide");
+      wide_z_ = wide_r_ = wide_xy_ = t == "wide";
+      tiles_source_ = t + "(fixed)";
+      return;
+    }
+    if (const char* env = std::getenv("SPO_B200_AUTOTUNE"))
+      if (std::string(env) == "0") return;
+    constexpr int reps = 3;
+    const double b = 0.0;
+    auto choose = [&](bool& flag, auto&& run) {
+      flag = false;
+      const float narrow = time_launches(run, reps);
+      flag = true;
+      const float wide = time_launches(run, reps);
+      flag = wide < 0.98f * narrow;  // keep the narrow tile unless the wide one is clearly faster
+    };
+    const bool was_on = prof_.on();
+    prof_.enable(false);
+    if (axis2_supported(s_.nz))
+      choose(wide_z_, [&] { axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zk_full_, wide_z_); });
+    if (axis2_supported(s_.nr))
+      choose(wide_r_, [&] { axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rk_full_, wide_r_); });
+    if (s_.nx == s_.ny && xy2_supported(s_.nx)) choose(wide_xy_, [&] { kinetic_xy(false, false); });
+    prof_.enable(was_on);
+    launches_ = 0;
+    tiles_source_ = "autotuned";
   }
 
   void axis(const char* name, double bytes, V* data, long long outer, const spo::FftPlan& plan, const V* tw,
@@ -921,8 +1126,138 @@ class Step final : public StepBase {
       }
       pot2_.identity_maps = identity ? 1 : 0;
     }
-    if (const char* env = std::getenv("SPO_B200_KERNELS")) use_v2_ = std::string(env) != "v1";
+    // The chunked potential kernel: one block per (point, chunk of pot3_cb_ columns), one thread per
+    // (column, theta) line, F and D in at most the device's opt-in shared memory.
+    pot3_cb_ = 0;
+    if (pot2_cb_ > 0 && s.nt <= 16 && 2 * s.mj_max + 1 <= s.nphi) {
+      std::vector<int> slot_first(s.nphi, 0), slot_nj(s.nphi, 0);
+      int jp = 1;
+      for (int b = 0; b < s.n_blocks; ++b) {
+        require(slot_nj[slot[b]] == 0, "two mJ blocks share a phi slot");
+        slot_first[slot[b]] = first[b];
+        slot_nj[slot[b]] = size[b];
+        jp = std::max(jp, size[b]);
+      }
+      const int cb = s.nt <= 4 ? 16 : 8;  // FP64 at cb = 32 spills; 16 columns keep 4+ warps per block
+      const std::size_t need = pot3_smem<T>(cb, jp, s.nt, s.nphi);
+      if (need <= static_cast<std::size_t>(smem_optin)) {
+        std::vector<double> leg_slot(static_cast<std::size_t>(s.nphi) * jp * s.nt, 0.0);
+        for (int b = 0; b < s.n_blocks; ++b)
+          for (int j = 0; j < size[b]; ++j)
+            for (int t = 0; t < s.nt; ++t)
+              leg_slot[(static_cast<std::size_t>(slot[b]) * jp + j) * s.nt + t] = legendre[offset[b] + t * size[b] + j];
+        pot3_cb_ = cb;
+        pot3_smem_ = need;
+        pot3_chunks_ = static_cast<int>((nxy + cb - 1) / cb);
+        pot3_args_ = pot2_;
+        pot3_args_.cb = cb;
+        pot3_args_.slot_first = upload_int(slot_first);
+        pot3_args_.slot_nj = upload_int(slot_nj);
+        pot3_args_.legendre_slot = upload_real(leg_slot);
+        pot3_args_.jp = jp;
+      }
+    }
+    // The persistent potential kernel with register-tiled contractions (ntheta 4, 8, 16; nphi 8, 16, 32).
+    pot4_kernel_ = (pot2_cb_ > 0 && 2 * s.mj_max + 1 <= s.nphi) ? pot4_kernel_for<T>(s.nphi, s.nt) : nullptr;
+    if (pot4_kernel_) {
+      const int cb = 128 / s.nt;
+      // Forward schedule: the slots in (+m, -m) pairs (m = 0 with an empty slot), pairs dealt to the four
+      // warps largest first, each to the least loaded warp; half-warp 2w takes the first of each pair
+      // of warp w, half-warp 2w + 1 the second.
+      std::vector<int> slot_first(s.nphi, 0), slot_nj(s.nphi, 0);
+      for (int b = 0; b < s.n_blocks; ++b) {
+        slot_first[slot[b]] = first[b];
+        slot_nj[slot[b]] = size[b];
+      }
+      struct Pair { int a, b, cost; };
+      std::vector<Pair> pairs;
+      std::vector<int> empty;
+      for (int p = 0; p < s.nphi; ++p)
+        if (slot_nj[p] == 0) empty.push_back(p);
+      std::size_t next_empty = 0;
+      auto take_empty = [&] { return next_empty < empty.size() ? empty[next_empty++] : -1; };
+      for (int m = 0; m <= s.mj_max; ++m) {
+        const int pa = m;                          // slot of +m
+        const int pb = m == 0 ? take_empty() : s.nphi - m;  // slot of -m
+        pairs.push_back({pa, pb, std::max(slot_nj[pa], pb >= 0 ? slot_nj[pb] : 0)});
+      }
+      while (next_empty < empty.size()) {
+        const int pa = take_empty();
+        pairs.push_back({pa, take_empty(), 0});
+      }
+      std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x.cost > y.cost; });
+      std::vector<std::vector<Pair>> warp(4);
+      std::vector<int> load(4, 0);
+      for (const Pair& pr : pairs) {
+        const int w = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+        warp[w].push_back(pr);
+        load[w] += pr.cost;
+      }
+      int len = 1;
+      for (const auto& w : warp) len = std::max<int>(len, static_cast<int>(w.size()));
+      std::vector<int> sched(8 * static_cast<std::size_t>(len), -1);
+      for (int w = 0; w < 4; ++w)
+        for (std::size_t k = 0; k < warp[w].size(); ++k) {
+          sched[(2 * w) * len + k] = warp[w][k].a;
+          sched[(2 * w + 1) * len + k] = warp[w][k].b;
+        }
+      std::vector<double> rows(static_cast<std::size_t>(s.n_rot) * (s.nt + 4), 0.0);
+      std::vector<int> irot_slot(s.n_rot);
+      for (int b = 0; b < s.n_blocks; ++b)
+        for (int j = 0; j < size[b]; ++j) {
+          irot_slot[first[b] + j] = slot[b];
+          for (int t = 0; t < s.nt; ++t)
+            rows[static_cast<std::size_t>(first[b] + j) * (s.nt + 4) + t] = legendre[offset[b] + t * size[b] + j];
+        }
+      pot4_smem_ = spo::pot4_smem<T>(s.n_rot, s.nphi, s.nt, cb, len);
+      if (pot4_smem_ <= static_cast<std::size_t>(smem_optin)) {
+        check_cuda(cudaFuncSetAttribute(pot4_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
+                   "potential4 smem");
+        int per_sm = 0, sms = 0;
+        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pot4_kernel_, 128, pot4_smem_),
+                   "potential4 occupancy");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
+        pot4_args_.p = pot2_.p;
+        pot4_args_.leg_rows = upload_real(rows);
+        pot4_args_.slot_first = upload_int(slot_first);
+        pot4_args_.slot_nj = upload_int(slot_nj);
+        pot4_args_.irot_slot = upload_int(irot_slot);
+        pot4_args_.fwd_sched = upload_int(sched);
+        pot4_args_.sched_len = len;
+        pot4_args_.chunks = static_cast<int>((nxy + cb - 1) / cb);
+        pot4_args_.n_items = static_cast<long long>(s.nzp) * s.nr * pot4_args_.chunks;
+        pot4_args_.identity_maps = pot2_.identity_maps;
+        pot4_blocks_ = static_cast<int>(std::min<long long>(static_cast<long long>(std::max(per_sm, 1)) * sms,
+                                                            std::max<long long>(pot4_args_.n_items, 1)));
+      } else {
+        pot4_kernel_ = nullptr;
+      }
+    }
+    if (pot3_cb_ > 0 || pot4_kernel_) {
+      require(sizeof(V) * (nxy + 1) <= static_cast<std::size_t>(smem_optin), "nx*ny too large for the projection kernel");
+      check_cuda(cudaFuncSetAttribute(spo::projection_finalize_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem_optin), "projection smem");
+    }
+    // The potential kernel is not chosen by timing: the kernels agree only to rounding (the compiler may
+    // contract the products of a complex multiply into FMAs differently in each), and a timing choice
+    // could then differ between two runs of the same case. The order is fixed: 4, 3, 2, general.
+    pot_kind_ = 1;
+    if (use_v2_ && pot2_cb_ > 0) pot_kind_ = 2;
+    if (use_v2_ && pot3_cb_ > 0) pot_kind_ = 3;
+    if (use_v2_ && pot4_kernel_) pot_kind_ = 4;
+    pot_source_ = "default";
+    if (const char* env = std::getenv("SPO_B200_KERNELS")) {
+      const std::string k(env);
+      require(k == "v1" || k == "v2" || k == "v3" || k == "v4", "SPO_B200_KERNELS must be v1, v2, v3 or v4");
+      use_v2_ = k != "v1";
+      const int want = k[1] - '0';
+      const bool have = want == 1 || (want == 2 && pot2_cb_ > 0) || (want == 3 && pot3_cb_ > 0) ||
+                        (want == 4 && pot4_kernel_ != nullptr);
+      pot_kind_ = have ? want : (use_v2_ && pot2_cb_ > 0 ? 2 : 1);
+      pot_source_ = "fixed";
+    }
     check_cuda(cudaStreamSynchronize(stream_), "set-up");
+    autotune();
   }
 
   // Host FP64 complex -> device T, through the staging buffer.
@@ -977,6 +1312,17 @@ class Step final : public StepBase {
   int pot2_cb_ = 0;
   std::size_t pot2_smem_ = 0;
   bool use_v2_ = true;  // register-DFT kernels where instantiated (SPO_B200_KERNELS=v1: the general kernels)
+  spo::Pot2Args<T> pot3_args_{};
+  int pot3_cb_ = 0, pot3_chunks_ = 0;
+  std::size_t pot3_smem_ = 0;
+  Pot4Kernel<T> pot4_kernel_ = nullptr;
+  spo::Pot4Args<T> pot4_args_{};
+  int pot4_blocks_ = 0;
+  std::size_t pot4_smem_ = 0;
+  int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4
+  std::string pot_source_ = "default";
+  bool wide_z_ = false, wide_r_ = false, wide_xy_ = false;
+  std::string tiles_source_ = "narrow";
   // Asymptotic analysis (FP64).
   std::vector<cplx> shift_host_;
   spo_analysis_desc an_{};
@@ -1026,6 +1372,7 @@ struct spo_handle {
   cudaStream_t stream = nullptr;
   Sizes s{};
   std::unique_ptr<StepBase> impl;
+  int ensembles = 0;  // live ensembles whose graphs hold this handle's device pointers
 };
 
 namespace {
@@ -1081,6 +1428,10 @@ int spo_create(const spo_desc* desc, spo_handle** out) {
 
 int spo_destroy(spo_handle* h) {
   if (!h) return SPO_OK;
+  if (h->ensembles > 0) {
+    h->err = "spo_destroy: the handle is a member of a live ensemble; destroy the ensemble first";
+    return SPO_ERR_STATE;
+  }
   cudaSetDevice(h->device);
   h->impl.reset();
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1189,6 +1540,141 @@ int spo_device_bytes(const spo_handle* h, unsigned long long* bytes) {
 int spo_last_launch_count(const spo_handle* h, int* launches) {
   if (!h || !launches) return SPO_ERR_INVALID;
   *launches = h->impl->launches();
+  return SPO_OK;
+}
+
+int spo_describe(const spo_handle* h, char* out, int out_len) {
+  if (!h || !out || out_len <= 0) return SPO_ERR_INVALID;
+  const std::string d = h->impl->describe();
+  const std::size_t n = std::min<std::size_t>(d.size(), static_cast<std::size_t>(out_len - 1));
+  std::memcpy(out, d.data(), n);
+  out[n] = '\0';
+  return SPO_OK;
+}
+
+int spo_averages(spo_handle* h, const double* z, const double* z_specular, const double* r, double volume_scattering,
+                 double volume_specular, int iz_analysis, int surface_index, double* out) {
+  return guarded(h, [&] {
+    h->impl->averages(z, z_specular, r, volume_scattering, volume_specular, iz_analysis, surface_index, out);
+  });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Ensembles: one analysis step of several handles captured as one CUDA graph, one branch per member
+// between a fork and a join, so that one graph launch runs every member's kernel sequence and the
+// independent members overlap on the GPU.
+// ---------------------------------------------------------------------------------------------
+struct spo_ensemble {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;
+  std::vector<spo_handle*> members;
+  ~spo_ensemble() {
+    for (spo_handle* m : members) --m->ensembles;
+    cudaSetDevice(device);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+extern "C" {
+
+const char* spo_ensemble_last_error(const spo_ensemble* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
+
+int spo_ensemble_create(spo_handle* const* members, int n_members, spo_ensemble** out) {
+  if (!out) return SPO_ERR_INVALID;
+  *out = nullptr;
+  auto e = std::make_unique<spo_ensemble>();
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> events;
+  bool capturing = false;
+  auto release = [&] {
+    for (cudaStream_t b : branch) cudaStreamDestroy(b);
+    for (cudaEvent_t ev : events) cudaEventDestroy(ev);
+    branch.clear();
+    events.clear();
+  };
+  try {
+    require(members != nullptr && n_members > 0, "spo_ensemble_create: no members");
+    for (int i = 0; i < n_members; ++i) {
+      require(members[i] != nullptr, "spo_ensemble_create: null member");
+      require(members[i]->device == members[0]->device, "spo_ensemble_create: members on different devices");
+      for (int k = 0; k < i; ++k) require(members[k] != members[i], "spo_ensemble_create: a member appears twice");
+    }
+    e->device = members[0]->device;
+    e->members.assign(members, members + n_members);
+    for (spo_handle* m : e->members) ++m->ensembles;
+    check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+    check_cuda(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    events.resize(n_members + 1, nullptr);
+    for (cudaEvent_t& ev : events) check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+    branch.resize(n_members, nullptr);
+    for (cudaStream_t& b : branch) check_cuda(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking), "cudaStreamCreate");
+    // Kernel profiling records events around each launch; a captured graph replays without them.
+    for (spo_handle* m : e->members) m->impl->profile(false);
+    check_cuda(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    capturing = true;
+    check_cuda(cudaEventRecord(events[0], e->stream), "cudaEventRecord");
+    for (int i = 0; i < n_members; ++i) {
+      StepBase& m = *e->members[i]->impl;
+      check_cuda(cudaStreamWaitEvent(branch[i], events[0], 0), "cudaStreamWaitEvent");
+      m.set_stream(branch[i]);
+      m.enqueue_analysis_step();
+      m.set_stream(nullptr);
+      e->launches += m.launches();
+      check_cuda(cudaEventRecord(events[i + 1], branch[i]), "cudaEventRecord");
+      check_cuda(cudaStreamWaitEvent(e->stream, events[i + 1], 0), "cudaStreamWaitEvent");
+    }
+    capturing = false;
+    check_cuda(cudaStreamEndCapture(e->stream, &e->graph), "cudaStreamEndCapture");
+    check_cuda(cudaGraphInstantiate(&e->exec, e->graph, 0), "cudaGraphInstantiate");
+  } catch (const std::exception& ex) {
+    if (capturing) {
+      cudaGraph_t partial = nullptr;
+      cudaStreamEndCapture(e->stream, &partial);
+      if (partial) cudaGraphDestroy(partial);
+    }
+    for (spo_handle* m : e->members) m->impl->set_stream(nullptr);
+    release();
+    g_create_error = ex.what();
+    const auto* se = dynamic_cast<const SpoError*>(&ex);
+    return se ? se->code : SPO_ERR_DEVICE;
+  }
+  release();
+  *out = e.release();
+  return SPO_OK;
+}
+
+int spo_ensemble_step(spo_ensemble* e) {
+  if (!e) return SPO_ERR_INVALID;
+  try {
+    check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+    check_cuda(cudaGraphLaunch(e->exec, e->stream), "cudaGraphLaunch");
+    check_cuda(cudaStreamSynchronize(e->stream), "spo_ensemble_step");
+    return SPO_OK;
+  } catch (const SpoError& ex) {
+    e->err = ex.what();
+    return ex.code;
+  } catch (const std::exception& ex) {
+    e->err = ex.what();
+    return SPO_ERR_DEVICE;
+  }
+}
+
+int spo_ensemble_launch_count(const spo_ensemble* e, int* launches) {
+  if (!e || !launches) return SPO_ERR_INVALID;
+  *launches = e->launches;
+  return SPO_OK;
+}
+
+int spo_ensemble_destroy(spo_ensemble* e) {
+  delete e;
   return SPO_OK;
 }
 

@@ -258,6 +258,7 @@ struct XyArgs {
   int nr;
   const T* opt_z;          // nz
   const Vec<T>* gas_step;  // (ir, irot): opt_r rot gas rot
+  int wide;                // launch choice of the register-DFT xy kernel: 32 rotational states per block
 };
 
 template <typename T>
@@ -620,6 +621,60 @@ __global__ void convert_kernel(const Vec<TI>* __restrict__ in, Vec<TO>* __restri
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
     const Vec<TI> v = in[i];
     out[i] = cmake<Vec<TO>>(static_cast<TO>(v.x), static_cast<TO>(v.y));
+  }
+}
+
+// Norm and position averages of the scattering plus specular wave in one block of 256 threads, FP64
+// (src/propagation/averages.cpp:37-80). grids = [z (nz) | z_specular (nzs) | r (nr)]; densities are
+// the block densities (izr = ir + nr iz). Seven sums, each strided per thread and then added in a
+// fixed tree: the scattering norm, Z and r moments, the same three on the specular grid, and the
+// specular norm between the analysis line (exclusive) and the analysis surface (inclusive).
+// out = {norm, <Z>, <r>, rest norm}.
+template <typename T>
+__global__ void __launch_bounds__(256) averages_kernel(const double* __restrict__ densities, const Vec<T>* __restrict__ chi,
+                                                       const double* __restrict__ grids, int nz, int nr, int nzs,
+                                                       int iz_analysis, int surface_index, double vol_scat,
+                                                       double vol_spec, double* __restrict__ out) {
+  __shared__ double part[7][256];
+  const double* zg = grids;
+  const double* zsg = grids + nz;
+  const double* rg = grids + nz + nzs;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  const int n_scat = nz * nr;
+  for (int izr = threadIdx.x; izr < n_scat; izr += blockDim.x) {
+    const double d = densities[izr];
+    acc[0] += d;
+    acc[1] += zg[izr / nr] * d;
+    acc[2] += rg[izr % nr] * d;
+  }
+  const int n_spec = nzs * nr;
+  for (int k = threadIdx.x; k < n_spec; k += blockDim.x) {
+    const int iz = k / nr;
+    const int ir = k - iz * nr;
+    const Vec<T> c = chi[k];
+    const double re = c.x, im = c.y;
+    const double d = re * re + im * im;
+    acc[3] += d;
+    acc[4] += zsg[iz] * d;
+    acc[5] += rg[ir] * d;
+    if (iz > iz_analysis && iz <= surface_index) acc[6] += d;
+  }
+#pragma unroll
+  for (int q = 0; q < 7; ++q) part[q][threadIdx.x] = acc[q];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+#pragma unroll
+      for (int q = 0; q < 7; ++q) part[q][threadIdx.x] += part[q][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double norm = part[0][0] * vol_scat + part[3][0] * vol_spec;
+    out[0] = norm;
+    out[1] = (part[1][0] * vol_scat + part[4][0] * vol_spec) / norm;
+    out[2] = (part[2][0] * vol_scat + part[5][0] * vol_spec) / norm;
+    out[3] = part[6][0] * vol_spec;
   }
 }
 

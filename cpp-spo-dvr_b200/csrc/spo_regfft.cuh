@@ -199,6 +199,7 @@ struct Axis2Args {
   long long inner;
   const Vec<T>* factor;  // N values, by k
   const Vec<T>* tw;      // N values: exp(-2 pi i j / N)
+  int wide;              // launch choice: 32 batch lanes per block where 16 is the default
 };
 
 // Dynamic shared memory: (N TB + 2 N) values (axis2_smem).
@@ -344,6 +345,12 @@ struct Pot2Args {
   const T* legendre_t;  // (block, J, theta)
   int cb;
   int identity_maps;    // no symmetry: representative = ixy and phi map = identity
+  // Slot-major forms for the chunked kernel: phi slot p holds mJ = p or p - nphi; its FBR states are
+  // slot_first[p] .. + slot_nj[p] (slot_nj = 0 for slots without basis functions); jp = max slot_nj.
+  const int* slot_first;
+  const int* slot_nj;
+  const T* legendre_slot;  // (p, j, theta), zero for j >= slot_nj[p]
+  int jp;
 };
 
 template <typename T, int NPHI, int CB>
@@ -465,6 +472,148 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
   const V proj = red[0];
   for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += blockDim.x)
     a.psi[(col_base + ixy) * n_rot + i0] = csub(i0buf[ixy], cmul(a.sp2sc[ixy], proj));
+}
+
+}  // namespace spo
+
+namespace spo {
+
+// ---------------------------------------------------------------------------------------------
+// Potential step of the interaction region, one block per (Z, r) point and chunk of CB (x, y)
+// columns (grid: chunks x points), one thread per (column, theta) line, no loop over chunks:
+//   load:    the chunk's columns (absorption, rot(dt/2), the specular wave into the initial channel),
+//            gathered slot-major into shared memory F[c][p][j]: phi slot p of mJ, its j-th FBR state,
+//            zero-padded to the longest mJ block (rows padded by 2 values against bank conflicts);
+//   forward: thread (c, theta) forms all NPHI phi slots at once, j by j, as NPHI independent FMA chains
+//            with the slot-major matrix (p, j, theta) through the read-only cache; DFT_NPHI (sign +1),
+//            times exp(i A) at the mapped phi, IDFT_NPHI (sign -1), into D[c][theta][p] (D reuses F);
+//   back:    thread j takes irot = j, j + blockDim.x, ...: theta sums for all CB columns with each matrix
+//            element loaded once, times rot(dt/2), stored;
+//   projection: projection_finalize_kernel, launched after this kernel, sums scattering_to_specular
+//            times the initial channel over all (x, y) columns of each point in column order
+//            (src/propagation/potential_operator.cpp:129-135) and subtracts the projection, so the
+//            result does not depend on the chunking.
+// ---------------------------------------------------------------------------------------------
+template <typename T, int NPHI, int CB>
+__global__ void __launch_bounds__(CB * 16) potential3_kernel(Pot2Args<T> args) {
+  using V = Vec<T>;
+  const PotArgs<T>& a = args.p;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n_rot = a.n_rot, nt = a.n_theta, jp = args.jp;
+  constexpr int LD = NPHI + 1;
+  const int FS = NPHI * jp + 2;                   // slot-major column stride, padded against bank conflicts
+  V* F = reinterpret_cast<V*>(smem_raw);          // CB * FS: F[c][p][j]
+  V* D = F;                                       // CB * nt * LD, after F is consumed
+  const int izr = blockIdx.y;
+  const int ir = izr % a.nr;
+  const int iz = izr / a.nr;
+  const int i0 = a.initial_channel;
+  const int c0 = blockIdx.x * CB;
+  const int ncol = min(CB, a.n_xy - c0);
+  const T oz = a.opt_z[iz];
+  const long long col_base = static_cast<long long>(izr) * a.n_xy + c0;
+  const int per_col = NPHI * jp;
+  for (int e = threadIdx.x; e < ncol * per_col; e += blockDim.x) {
+    const int c = e / per_col;
+    const int r = e - c * per_col;
+    const int p = r / jp;
+    const int j = r - p * jp;
+    V v = cmake<V>(0, 0);
+    if (j < __ldg(args.slot_nj + p)) {
+      const int irot = __ldg(args.slot_first + p) + j;
+      v = a.psi[(col_base + c) * n_rot + irot];
+      v = cscale(cmul(a.before[ir * n_rot + irot], v), oz);
+      if (irot == i0) {
+        const V incoming = a.chi[ir + a.nr * iz];
+        v = cadd(v, cmul(a.rot_half[ir * n_rot + i0], cmul(a.sp2sc[c0 + c], incoming)));
+      }
+    }
+    F[c * FS + r] = v;
+  }
+  __syncthreads();
+  const int line_c = threadIdx.x / nt;
+  const int line_t = threadIdx.x - line_c * nt;
+  const bool has_line = line_c < ncol;
+  V x[NPHI];
+  if (has_line) {
+    const V* f = F + line_c * FS;
+    const T* mt = args.legendre_slot + line_t;
+    static_for<0, NPHI>([&](auto p) { x[p] = cmake<V>(0, 0); });
+    for (int j = 0; j < jp; ++j) {
+      static_for<0, NPHI>([&](auto p) {
+        constexpr int P = SPO_CV(p);
+        const T w = __ldg(mt + (P * jp + j) * nt);
+        const V fv = f[P * jp + j];
+        x[P] = cmake<V>(x[P].x + w * fv.x, x[P].y + w * fv.y);
+      });
+    }
+  }
+  __syncthreads();  // F is consumed; D takes its memory
+  if (has_line) {
+    const int ixy = c0 + line_c;
+    rdft<NPHI, +1>(x);
+    if (args.identity_maps) {
+      const V* e = a.expia + (static_cast<long long>(izr) * a.n_rep + ixy) * nt * NPHI + line_t * NPHI;
+      static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + p), x[p]); });
+    } else {
+      const V* e = a.expia + (static_cast<long long>(izr) * a.n_rep + a.rep_of[ixy]) * nt * NPHI + line_t * NPHI;
+      const int* map = a.phi_map + ixy * NPHI;
+      static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + __ldg(map + p)), x[p]); });
+    }
+    rdft<NPHI, -1>(x);
+    static_for<0, NPHI>([&](auto p) { D[(line_c * nt + line_t) * LD + p] = x[p]; });
+  }
+  __syncthreads();
+  for (int irot = threadIdx.x; irot < n_rot; irot += blockDim.x) {
+    const int blk = __ldg(a.irot_block + irot);
+    const int nj = __ldg(a.block_size + blk);
+    const int jj = irot - __ldg(a.block_first + blk);
+    const int slot = __ldg(a.block_slot + blk);
+    const T* col = a.legendre + __ldg(a.block_offset + blk) + jj;  // (theta, J) within the block
+    V acc[CB];
+#pragma unroll
+    for (int c = 0; c < CB; ++c) acc[c] = cmake<V>(0, 0);
+    for (int t = 0; t < nt; ++t) {
+      const T w = __ldg(col + t * nj);
+      const V* d = D + t * LD + slot;
+#pragma unroll
+      for (int c = 0; c < CB; ++c) {
+        const V dv = d[c * nt * LD];
+        acc[c] = cmake<V>(acc[c].x + w * dv.x, acc[c].y + w * dv.y);
+      }
+    }
+    const V rh = a.rot_half[ir * n_rot + irot];
+#pragma unroll
+    for (int c = 0; c < CB; ++c)
+      if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, acc[c]);
+  }
+}
+
+// The projection of each interaction-region point onto the specular grid
+// (src/propagation/potential_operator.cpp:129-135): chi(ir, iz) = sum over the (x, y) columns, in column
+// order, of scattering_to_specular times the initial channel, then specular_to_scattering times it
+// subtracted from the initial channel of every column. One block per point; the initial channel of the
+// point's columns is gathered into shared memory (n_xy values) and summed by one thread.
+template <typename T>
+__global__ void projection_finalize_kernel(Vec<T>* __restrict__ psi, Vec<T>* __restrict__ chi, int n_rot, int n_xy,
+                                           int i0, const Vec<T>* __restrict__ sc2sp, const Vec<T>* __restrict__ sp2sc) {
+  using V = Vec<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* col = reinterpret_cast<V*>(smem_raw);  // n_xy
+  V& proj = col[n_xy];                      // dynamic shared memory: (n_xy + 1) values
+  const long long base = static_cast<long long>(blockIdx.x) * n_xy;  // blockIdx.x = ir + nr iz
+  for (int ixy = threadIdx.x; ixy < n_xy; ixy += blockDim.x) col[ixy] = psi[(base + ixy) * n_rot + i0];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    V p = cmake<V>(0, 0);
+    for (int ixy = 0; ixy < n_xy; ++ixy) p = cadd(p, cmul(sc2sp[ixy], col[ixy]));
+    proj = p;
+    chi[blockIdx.x] = p;
+  }
+  __syncthreads();
+  const V p = proj;
+  for (int ixy = threadIdx.x; ixy < n_xy; ixy += blockDim.x)
+    psi[(base + ixy) * n_rot + i0] = csub(col[ixy], cmul(sp2sc[ixy], p));
 }
 
 }  // namespace spo

@@ -4,7 +4,7 @@ The compute path is the C ABI of include/spo_b200.h (lib/libspo_b200.so); this p
 side: the PropagationBackend-shaped wrapper, case bundles and the benchmark's synthetic workloads.
 """
 
-from .backend import B200Backend  # noqa: F401
+from .backend import B200Backend, Ensemble  # noqa: F401
 from .capi import B200Error  # noqa: F401
 from .case import CaseBundle  # noqa: F401
 

@@ -10,6 +10,7 @@ member, with the same layouts (src/propagation/wave_function.hpp) and the same m
   z_plane(iz) ..................... PropagationBackend::z_plane
   block_densities() ............... PropagationBackend::block_densities
   site_column(ixy) ................ PropagationBackend::site_column
+  averages(...) ................... compute_averages (src/propagation/averages.cpp:37-80) on the device
 
 Errors: the reference throws (InputError, CudaError); here a non-zero status raises B200Error
 carrying the library's message. Construction takes a CaseBundle, the file form of BackendInput +
@@ -86,7 +87,9 @@ class B200Backend:
     # ------------------------------------------------------------------ lifetime
     def close(self):
         if getattr(self, "_h", None):
-            self._lib.spo_destroy(self._h)
+            st = self._lib.spo_destroy(self._h)
+            if st != capi.SPO_OK:  # a member of a live ensemble
+                raise capi.B200Error(st, self._lib.spo_last_error(self._h).decode())
             self._h = None
 
     def __del__(self):
@@ -216,3 +219,69 @@ class B200Backend:
         v = ctypes.c_int()
         self._check(self._lib.spo_last_launch_count(self._h, ctypes.byref(v)))
         return v.value
+
+    def describe(self) -> str:
+        """The kernels and tile widths this handle uses, and whether the autotuner chose them."""
+        buf = ctypes.create_string_buffer(512)
+        self._check(self._lib.spo_describe(self._h, buf, 512))
+        return buf.value.decode()
+
+    def averages(self, z: np.ndarray, z_specular: np.ndarray, r: np.ndarray, volume_scattering: float,
+                 volume_specular: float, iz_analysis: int, surface_index: int) -> np.ndarray:
+        """[norm, <Z>, <r>, rest norm] of the resident wave packet, in FP64 on the device."""
+        z, zs, r = _f(z), _f(z_specular), _f(r)
+        if len(z) != self.case.nz or len(zs) != self.case.nz_specular or len(r) != self.case.nr:
+            raise ValueError("averages: grid lengths must be nz, nz_specular and nr")
+        out = np.empty(4)
+        self._check(self._lib.spo_averages(self._h, capi.dptr(z), capi.dptr(zs), capi.dptr(r),
+                                           float(volume_scattering), float(volume_specular), int(iz_analysis),
+                                           int(surface_index), capi.dptr(out)))
+        return out
+
+
+class Ensemble:
+    """Several B200Backend wave packets advanced together: one analysis step of every member is one
+    CUDA graph launch (spo_ensemble_* of include/spo_b200.h). Members may differ in grid sizes and
+    precision; each keeps its own state and stays usable on its own between ensemble steps."""
+
+    def __init__(self, members: list[B200Backend]):
+        if not members:
+            raise ValueError("an ensemble needs at least one member")
+        self._lib = capi.lib()
+        self.members = list(members)  # the graph holds their device pointers: keep them alive
+        arr = (ctypes.c_void_p * len(self.members))(*[m._h for m in self.members])
+        e = ctypes.c_void_p()
+        status = self._lib.spo_ensemble_create(arr, len(self.members), ctypes.byref(e))
+        if status != 0:
+            raise capi.B200Error(status, self._lib.spo_ensemble_last_error(None).decode())
+        self._e = e
+
+    def _check(self, status: int):
+        if status != 0:
+            raise capi.B200Error(status, self._lib.spo_ensemble_last_error(self._e).decode())
+
+    def propagate_analysis_step(self) -> None:
+        """One analysis step of every member (one graph launch); returns when all are done."""
+        self._check(self._lib.spo_ensemble_step(self._e))
+
+    def launch_count(self) -> int:
+        v = ctypes.c_int()
+        self._check(self._lib.spo_ensemble_launch_count(self._e, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_e", None):
+            self._lib.spo_ensemble_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

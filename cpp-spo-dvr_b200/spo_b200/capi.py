@@ -28,6 +28,8 @@ EXPORTS = [
     "spo_block_densities", "spo_site_column", "spo_apply_stage", "spo_set_stream", "spo_profile",
     "spo_profile_count", "spo_profile_entry", "spo_device_bytes", "spo_last_launch_count",
     "spo_block_densities_noalloc", "spo_analysis_setup", "spo_bk_coefficients", "spo_s_matrix_sums",
+    "spo_describe", "spo_averages", "spo_ensemble_create", "spo_ensemble_step", "spo_ensemble_launch_count",
+    "spo_ensemble_last_error", "spo_ensemble_destroy",
 ]
 NOALLOC_MAX_BLOCKS = 65536
 
@@ -109,8 +111,17 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.spo_block_densities_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong,
                                                 _dp, ctypes.c_void_p]
     lib.spo_last_launch_count.argtypes = [h, _ip]
+    lib.spo_describe.argtypes = [h, ctypes.c_char_p, ctypes.c_int]
+    lib.spo_averages.argtypes = [h, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
+    e = ctypes.c_void_p
+    lib.spo_ensemble_create.argtypes = [ctypes.POINTER(h), ctypes.c_int, ctypes.POINTER(e)]
+    lib.spo_ensemble_step.argtypes = [e]
+    lib.spo_ensemble_launch_count.argtypes = [e, _ip]
+    lib.spo_ensemble_last_error.argtypes = [e]
+    lib.spo_ensemble_last_error.restype = ctypes.c_char_p
+    lib.spo_ensemble_destroy.argtypes = [e]
     for name in EXPORTS:
-        if name not in ("spo_version", "spo_last_error"):
+        if name not in ("spo_version", "spo_last_error", "spo_ensemble_last_error"):
             getattr(lib, name).restype = ctypes.c_int
     return lib
 

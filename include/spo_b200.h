@@ -113,7 +113,8 @@ const char* spo_last_error(const spo_handle* h);
  * (src/propagation/cpu_backend.cpp:24-44) behind BackendFactory (propagation_backend.hpp:73-74). */
 int spo_create(const spo_desc* desc, spo_handle** out);
 
-/* Frees the handle and all its device memory. */
+/* Frees the handle and all its device memory. Refused with SPO_ERR_STATE while the handle is a
+ * member of a live ensemble (whose graph holds its device pointers). */
 int spo_destroy(spo_handle* h);
 
 /* [T(dt/2) V(dt) T(dt/2)]^n over one analysis step, n = steps_per_analysis.
@@ -218,6 +219,47 @@ int spo_device_bytes(const spo_handle* h, unsigned long long* bytes);
 
 /* Number of kernel launches the last spo_propagate_analysis_step issued. */
 int spo_last_launch_count(const spo_handle* h, int* launches);
+
+/* The kernels and tile shapes the handle chose (kernel per pass, tile width per kinetic pass, and
+ * whether the autotuner or an environment setting chose them), as one NUL-terminated line truncated
+ * to out_len bytes. No counterpart in the reference (its CUDA backend has one fixed plan). */
+int spo_describe(const spo_handle* h, char* out, int out_len);
+
+/* Norm and position averages of the resident wave packet, computed on the device in FP64:
+ * out[0] = norm (scattering plus specular grid), out[1] = <Z>, out[2] = <r>, out[3] = the specular
+ * norm between the analysis line iz_analysis (exclusive) and the analysis surface surface_index
+ * (inclusive). z (nz), z_specular (nz_specular), r (nr): the grids; volume_scattering = dZ dr times
+ * the xy volume element, volume_specular = dZ dr. Replaces compute_averages
+ * (src/propagation/averages.hpp:29-30, averages.cpp:37-80) on the backend's block densities and
+ * specular wave. */
+int spo_averages(spo_handle* h, const double* z, const double* z_specular, const double* r, double volume_scattering,
+                 double volume_specular, int iz_analysis, int surface_index, double* out);
+
+/* ---------------------------------------------------------------------------------------------
+ * Ensembles of wave packets (no counterpart in the reference, which propagates one wave packet per
+ * run): one analysis step of every member handle, captured once as one CUDA graph with one branch per
+ * member, so that one graph launch advances all of them and members of uneven grid sizes overlap on
+ * the GPU. Members keep their own state, tables and precision and stay usable one by one (a member's
+ * analysis, download, upload between ensemble steps); each ensemble step gives every member exactly
+ * the state that spo_propagate_analysis_step on that member alone gives.
+ *
+ * All members must live on one device; they must outlive the ensemble. spo_ensemble_create switches
+ * the members' kernel profiling off and returns them to their own streams.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct spo_ensemble spo_ensemble;
+
+int spo_ensemble_create(spo_handle* const* members, int n_members, spo_ensemble** out);
+
+/* One analysis step of every member (one graph launch); returns when all are done. */
+int spo_ensemble_step(spo_ensemble* e);
+
+/* Kernel launches in one ensemble step (the sum over the members). */
+int spo_ensemble_launch_count(const spo_ensemble* e, int* launches);
+
+/* Message of the last failed call on e (of the last failed spo_ensemble_create when e is NULL). */
+const char* spo_ensemble_last_error(const spo_ensemble* e);
+
+int spo_ensemble_destroy(spo_ensemble* e);
 
 /* ---------------------------------------------------------------------------------------------
  * Block densities without any device allocation.

@@ -373,6 +373,21 @@ int run_case(const Options& o) {
   const spodvr::WavePacket& psi = backend->wave_packet_on_host();
   if (o.dump_psi) write_vec(o.out / "psi_final.c128", std::vector<cplx>(psi.scattering.values.begin(), psi.scattering.values.end()));
   write_vec(o.out / "block_densities.f64", backend->block_densities());
+  // The averages of the final wave packet (src/propagation/averages.cpp:37-80) with their inputs.
+  {
+    const double time = times.empty() ? p.t_end : times.back();
+    const spodvr::Averages av = spodvr::compute_averages(time, psi, config, *s.grids, surface.index());
+    write_vec(o.out / "averages.f64", std::vector<double>{av.norm, av.z_mean, av.r_mean, av.rest_norm});
+    write_vec(o.out / "grid_z.f64", std::vector<double>(s.grids->z_scattering.points().begin(), s.grids->z_scattering.points().end()));
+    write_vec(o.out / "grid_z_specular.f64", std::vector<double>(s.grids->z_specular.points().begin(), s.grids->z_specular.points().end()));
+    write_vec(o.out / "grid_r.f64", std::vector<double>(s.grids->r.points().begin(), s.grids->r.points().end()));
+    json g;
+    g["volume_scattering"] = p.dz * p.dr * config.derived.xy_volume_element;
+    g["volume_specular"] = p.dz * p.dr;
+    g["iz_analysis"] = s.grids->iz_analysis;
+    g["surface_index"] = surface.index();
+    std::ofstream(o.out / "averages.json") << g.dump(1);
+  }
   const spodvr::ScatteringResults results = s_matrix.results(surface.fixed_line());
   std::vector<double> p_reaction;
   for (const auto& e : results.energies) p_reaction.push_back(e.p_reaction);

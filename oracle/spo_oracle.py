@@ -15,6 +15,7 @@ It restates, operator by operator, what the reference's CPU backend does in one 
 * ``fbr_to_dvr`` / ``dvr_to_fbr`` .. src/propagation/angular_transform.cpp:54-114
 * ``bk_coefficients`` .............. src/analysis/balint_kurti.cpp:39-84
 * ``block_densities`` .............. src/propagation/averages.cpp:20-29
+* ``averages`` ..................... src/propagation/averages.cpp:37-80
 
 Its inputs are a *case bundle*: the data that cross the reference's PropagationBackend boundary
 (src/propagation/propagation_backend.hpp:63-74: the tables, the angular transform matrices, the
@@ -293,6 +294,29 @@ def block_densities(psi: np.ndarray) -> np.ndarray:
     """sum |psi|^2 over (irot, ixy) per (Z, r) point (averages.cpp:20-29), izr = ir + nr*iz."""
     nz, nr = psi.shape[:2]
     return np.sum(np.abs(psi.reshape(nz * nr, -1)) ** 2, axis=1)
+
+
+def averages(densities: np.ndarray, chi: np.ndarray, z: np.ndarray, z_specular: np.ndarray, r: np.ndarray,
+             volume_scattering: float, volume_specular: float, iz_analysis: int, surface_index: int) -> np.ndarray:
+    """Norm and position averages (averages.cpp:37-80): [norm, <Z>, <r>, rest norm].
+
+    densities: block densities, izr = ir + nr*iz; chi: (nz_specular, nr). The norm is the scattering
+    plus the specular norm, each times its volume element; <Z> and <r> divide the summed moments by
+    it; the rest norm is the specular norm of iz_analysis < iz <= surface_index (times dZ dr).
+    """
+    nr = len(r)
+    nz = len(densities) // nr
+    d = np.asarray(densities, dtype=np.float64).reshape(nz, nr)
+    c2 = np.abs(np.asarray(chi).reshape(len(z_specular), nr)) ** 2
+    norm_scat = d.sum() * volume_scattering
+    z_scat = (np.asarray(z)[:nz, None] * d).sum() * volume_scattering
+    r_scat = (np.asarray(r)[None, :] * d).sum() * volume_scattering
+    norm_spec = c2.sum() * volume_specular
+    z_spec = (np.asarray(z_specular)[:, None] * c2).sum() * volume_specular
+    r_spec = (np.asarray(r)[None, :] * c2).sum() * volume_specular
+    rest = c2[iz_analysis + 1:surface_index + 1].sum() * volume_specular
+    norm = norm_scat + norm_spec
+    return np.array([norm, (z_scat + z_spec) / norm, (r_scat + r_spec) / norm, rest])
 
 
 def bk_coefficients(z_plane: np.ndarray, chi: np.ndarray, case: Case, surface_fixed: bool,

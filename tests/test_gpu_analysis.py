@@ -59,3 +59,31 @@ def test_bk_and_s_matrix_match_the_reference_analysis(ref_case, name, precision)
     ref_sums = O.s_matrix_sums(ref_bk, times, energies, a["analysis_time_step"])
     assert np.max(np.abs(sums - ref_sums)) <= tol * np.max(np.abs(ref_sums))
     be.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_averages_match_the_oracle(precision):
+    """spo_averages (norm, <Z>, <r>, rest norm on the device) against compute_averages restated in the
+    oracle (averages.cpp:37-80), on a random wave packet: FP64 sums in another order, so 1e-12; the
+    mixed form holds the state in complex64, so its inputs differ by the rounding of psi (2e-6)."""
+    from spo_b200 import B200Backend, workload
+    case = workload.config_case({"nz": 48, "nr": 24, "nx": 4, "ny": 4, "j_max": 3, "mj_max": 3,
+                                 "nz_specular": 96, "nz_potential": 30})
+    rng = np.random.default_rng(21)
+    psi = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    z = 1.5 + 0.12 * np.arange(case.nz)
+    zs = 1.5 + 0.12 * np.arange(case.nz_specular)
+    r = 0.4 + 0.1 * np.arange(case.nr)
+    vol_scat, vol_spec = 0.12 * 0.1 * 0.37, 0.12 * 0.1
+    iz_analysis, surface = 30, 70
+    with B200Backend(case, precision=precision) as be:
+        be.read_wave_packet(psi, chi)
+        got = be.averages(z, zs, r, vol_scat, vol_spec, iz_analysis, surface)
+        dens = be.block_densities()
+        psi_dev, chi_dev = be.wave_packet_on_host()
+    ref = O.averages(dens, chi_dev, z, zs, r, vol_scat, vol_spec, iz_analysis, surface)
+    assert np.max(np.abs(got - ref) / np.abs(ref)) <= 1e-12
+    exact = O.averages(O.block_densities(psi), chi, z, zs, r, vol_scat, vol_spec, iz_analysis, surface)
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    assert np.max(np.abs(got - exact) / np.abs(exact)) <= tol

@@ -2,10 +2,19 @@
 (needs a B200).
 
 The tiny regression cases (test_gpu_parity.py) run the register-DFT kernels at their own sizes
-against the oracle. The configuration-2 sizes (axis lengths 128 = 16 x 8 and 48 = 8 x 6, a 16 x 16
+against the oracle. The configuration-2 sizes (axis lengths 128 = 8 x 16 and 48 = 6 x 8, a 16 x 16
 (x, y) grid, nphi 32 with ntheta 16) use other instantiations; here they are checked operator by
 operator and over an analysis step against the general shared-memory Stockham kernels
-(SPO_B200_KERNELS=v1), which the oracle checks on every case.
+(SPO_B200_KERNELS=v1), which the oracle checks on every case. All register potential kernels are
+covered: v2 (potential2, one block per (Z, r) point looping over column chunks), v3 (potential3, one
+block per point and chunk) and v4 (potential4, persistent blocks with register-tiled theta
+contractions). v3 and v4 apply the same operations in the same order to every column and leave the
+projection to a second kernel; they agree to rounding (not bitwise: the compiler may contract the
+products of a complex multiply into FMAs differently in each kernel).
+
+The narrow and wide tiles of the register kernels compute every line with the same operations in the
+same order, so the two give bitwise equal wave packets; the autotuner's choice between them can
+change the speed only.
 """
 
 import os
@@ -26,22 +35,29 @@ SHAPES = {
 }
 
 
-def make(case, kernels, precision):
+def make(case, kernels, precision, tiles=None):
     from spo_b200 import B200Backend
-    old = os.environ.get("SPO_B200_KERNELS")
-    os.environ["SPO_B200_KERNELS"] = kernels
+    env = {"SPO_B200_KERNELS": kernels, "SPO_B200_TILES": tiles}
+    old = {k: os.environ.get(k) for k in env}
+    for k, v in env.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
     try:
         return B200Backend(case, precision=precision)
     finally:
-        if old is None:
-            del os.environ["SPO_B200_KERNELS"]
-        else:
-            os.environ["SPO_B200_KERNELS"] = old
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
 
 
 @pytest.mark.parametrize("shape", list(SHAPES))
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_register_kernels_match_general_kernels(shape, precision):
+@pytest.mark.parametrize("kernels", ["v2", "v3", "v4"])
+def test_register_kernels_match_general_kernels(shape, precision, kernels):
     from spo_b200 import capi, workload
     case = workload.config_case(SHAPES[shape])
     rng = np.random.default_rng(5)
@@ -49,7 +65,8 @@ def test_register_kernels_match_general_kernels(shape, precision):
     chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
     tol_stage, tol_step = (1e-12, 1e-11) if precision == "fp64" else (2e-6, 2e-5)
     ref = make(case, "v1", precision)
-    new = make(case, "v2", precision)
+    new = make(case, kernels, precision)
+    assert f"potential=potential{kernels[1]}" in new.describe(), new.describe()
     for be in (ref, new):
         be.read_wave_packet(psi0, chi0)
     for stage in (capi.STAGE_ZR, capi.STAGE_XY, capi.STAGE_POTENTIAL):
@@ -67,3 +84,46 @@ def test_register_kernels_match_general_kernels(shape, precision):
     assert rel_l2(p2, p1) < tol_step and rel_l2(c2, c1) < tol_step
     ref.close()
     new.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_narrow_and_wide_tiles_are_bitwise_equal(precision):
+    from spo_b200 import workload
+    # Z 128 = 8 x 16 and (x, y) 16 x 16: the lengths whose kernels have both tiles
+    case = workload.config_case({"nz": 128, "nr": 24, "nx": 16, "ny": 16, "j_max": 3, "mj_max": 3,
+                                 "nz_specular": 256, "nz_potential": 40})
+    rng = np.random.default_rng(9)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    out = []
+    for tiles in ("narrow", "wide"):
+        be = make(case, "v3", precision, tiles)
+        assert tiles in be.describe(), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("j_max", [15, 7, 3])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_potential3_and_potential4_agree(j_max, precision):
+    """ntheta 16 / nphi 32, ntheta 8 / nphi 16 and ntheta 4 / nphi 8: every instantiation family of
+    potential4 against potential3 over an analysis step, to rounding (1e-13 FP64, 2e-6 mixed)."""
+    from spo_b200 import workload
+    case = workload.config_case({"nz": 32, "nr": 24, "nx": 8, "ny": 8, "j_max": j_max, "mj_max": j_max,
+                                 "nz_specular": 64, "nz_potential": 20})
+    rng = np.random.default_rng(3)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    out = []
+    for kernels in ("v3", "v4"):
+        be = make(case, kernels, precision)
+        assert f"potential=potential{kernels[1]}" in be.describe(), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    tol = 1e-13 if precision == "fp64" else 2e-6
+    assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol

@@ -92,3 +92,21 @@ def test_restatement_matches_reference_build(ref_case, name):
     assert rel_err(chi, chis[1]) < tol
     dens = np.fromfile(os.path.join(d, "block_densities.f64"))
     assert np.max(np.abs(O.block_densities(p) - dens)) <= 1e-13 * np.max(dens)
+
+
+@pytest.mark.parametrize("name", ["tiny_dailight", "tiny_oblique"])
+def test_averages_restatement_matches_reference_build(ref_case, name):
+    """The oracle's averages against the reference's compute_averages (averages.cpp:37-80) on the final
+    wave packet of two analysis steps, with the reference's own densities, grids and volume elements."""
+    import json
+    d = ref_case(name)
+    case = O.load_case(os.path.join(d, "case"))
+    g = json.load(open(os.path.join(d, "averages.json")))
+    ref = np.fromfile(os.path.join(d, "averages.f64"))
+    chis = read_c128(os.path.join(d, "chi_steps.c128"), (2, case.nz_specular, case.nr))
+    got = O.averages(np.fromfile(os.path.join(d, "block_densities.f64")), chis[1],
+                     np.fromfile(os.path.join(d, "grid_z.f64")), np.fromfile(os.path.join(d, "grid_z_specular.f64")),
+                     np.fromfile(os.path.join(d, "grid_r.f64")), g["volume_scattering"], g["volume_specular"],
+                     g["iz_analysis"], g["surface_index"])
+    assert ref[3] > 0.0  # the rest-norm window is not empty
+    assert np.max(np.abs(got - ref) / np.abs(ref)) <= 1e-13
