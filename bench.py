@@ -292,7 +292,9 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "kernels_mixed": m["kernels"], "kernels_fp64": res["fp64"]["kernels"]},
             "fp64": {"value": out["fp64"]["value"], "ms_per_step": out["fp64"]["ms"] / args.steps,
-                     "e2e": out["fp64"]["e2e"]},
+                     "e2e": out["fp64"]["e2e"],
+                     "kernels": [{"name": r["name"], "launches": r["launches"],
+                                  "avg_ms": round(r["ms"] / r["launches"], 5)} for r in res["fp64"]["records"]]},
             "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
             "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,

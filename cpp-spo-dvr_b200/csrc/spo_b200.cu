@@ -168,14 +168,18 @@ bool launch_axis2_tb(const spo::Axis2Args<T>& a, long long outer, cudaStream_t s
   return true;
 }
 
-// Tile width (batch lanes per block): 32 lanes when a line has at most 8 sub-rows; for 16 sub-rows
-// 16 lanes (256 threads) or, when the autotuner chose it (wide), 32 lanes (512 threads).
+// Tile width (batch lanes per block): 32 lanes when a line has at most 8 sub-rows; for more sub-rows
+// 16 lanes by default, or 8 or 32 lanes as the autotuner chose.
 template <typename T, int N1, int N2>
 bool launch_axis2_n(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
   constexpr int NS = N1 > N2 ? N1 : N2;
-  if constexpr (NS <= 8) return launch_axis2_tb<T, N1, N2, 32>(a, outer, stream);
-  else if (a.wide) return launch_axis2_tb<T, N1, N2, 32>(a, outer, stream);
-  else return launch_axis2_tb<T, N1, N2, 16>(a, outer, stream);
+  if constexpr (NS <= 8) {
+    return launch_axis2_tb<T, N1, N2, 32>(a, outer, stream);
+  } else {
+    if (a.tile == 8) return launch_axis2_tb<T, N1, N2, 8>(a, outer, stream);
+    if (a.tile == 32) return launch_axis2_tb<T, N1, N2, 32>(a, outer, stream);
+    return launch_axis2_tb<T, N1, N2, 16>(a, outer, stream);
+  }
 }
 
 template <typename T>
@@ -197,6 +201,13 @@ bool launch_axis2(int n, const spo::Axis2Args<T>& a, long long outer, cudaStream
     case 192: return launch_axis2_n<T, 12, 16>(a, outer, stream);
     case 224: return launch_axis2_n<T, 14, 16>(a, outer, stream);
     case 256: return launch_axis2_n<T, 16, 16>(a, outer, stream);
+    default: return false;
+  }
+}
+// Lengths whose register kernel has more than 8 sub-rows, i.e. a choice of tile widths.
+bool axis2_has_tiles(int n) {
+  switch (n) {
+    case 80: case 96: case 112: case 128: case 160: case 176: case 192: case 224: case 256: return true;
     default: return false;
   }
 }
@@ -223,9 +234,13 @@ void launch_xy2_tb(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream)
 template <typename T, int NX, int NY>
 void launch_xy2_n(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream) {
   constexpr int NS = NX > NY ? NX : NY;
-  if constexpr (NS <= 8) launch_xy2_tb<T, NX, NY, 32>(a, n_zr, stream);
-  else if (a.wide) launch_xy2_tb<T, NX, NY, 32>(a, n_zr, stream);
-  else launch_xy2_tb<T, NX, NY, 16>(a, n_zr, stream);
+  if constexpr (NS <= 8) {
+    launch_xy2_tb<T, NX, NY, 32>(a, n_zr, stream);
+  } else {
+    if (a.tile == 8) launch_xy2_tb<T, NX, NY, 8>(a, n_zr, stream);
+    else if (a.tile == 32) launch_xy2_tb<T, NX, NY, 32>(a, n_zr, stream);
+    else launch_xy2_tb<T, NX, NY, 16>(a, n_zr, stream);
+  }
 }
 
 template <typename T>
@@ -467,15 +482,16 @@ class Step final : public StepBase {
   }
 
   std::string describe() const override {
-    auto axis_name = [&](int n, bool wide) {
+    auto lanes = [](int tile, bool has_tiles) { return "tb" + std::to_string(!has_tiles ? 32 : tile ? tile : 16); };
+    auto axis_name = [&](int n, int tile) {
       if (!(use_v2_ && axis2_supported(n))) return std::string("axis_pass(general)");
-      return "axis2<" + std::to_string(n) + (wide ? ",wide>" : ",narrow>");
+      return "axis2<" + std::to_string(n) + "," + lanes(tile, axis2_has_tiles(n)) + ">";
     };
     std::string out = std::string(sizeof(T) == 8 ? "fp64" : "mixed");
-    out += " z=" + axis_name(s_.nz, wide_z_);
-    out += " r=" + axis_name(s_.nr, wide_r_);
+    out += " z=" + axis_name(s_.nz, tile_z_);
+    out += " r=" + axis_name(s_.nr, tile_r_);
     const bool xy2 = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx);
-    out += std::string(" xy=") + (xy2 ? "xy2<" + std::to_string(s_.nx) + (wide_xy_ ? ",wide>" : ",narrow>")
+    out += std::string(" xy=") + (xy2 ? "xy2<" + std::to_string(s_.nx) + "," + lanes(tile_xy_, s_.nx > 8) + ">"
                                       : std::string("xy_pass(general)"));
     if (pot_kind_ == 4)
       out += " potential=potential4<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
@@ -686,16 +702,16 @@ class Step final : public StepBase {
   // T_Z and T_r of the scattering wave.
   void kinetic_zr(bool half) {
     const double b = 2.0 * sizeof(V) * s_.n_psi();
-    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, wide_z_);
-    axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, wide_r_);
+    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, tile_z_);
+    axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, tile_r_);
   }
 
   // A kinetic axis pass over psi: the register-DFT kernel for its length when instantiated, else the
   // general Stockham kernel.
   void axis_psi(const char* name, double bytes, long long outer, const spo::FftPlan& plan, const V* tw,
-                long long inner, const V* factor, bool wide) {
+                long long inner, const V* factor, int tile) {
     if (use_v2_ && axis2_supported(plan.n)) {
-      spo::Axis2Args<T> a{psi_, inner, factor, tw, wide ? 1 : 0};
+      spo::Axis2Args<T> a{psi_, inner, factor, tw, tile};
       prof_.begin(stream_);
       launch_axis2<T>(plan.n, a, outer, stream_);
       prof_.end(stream_, name, bytes);
@@ -725,7 +741,7 @@ class Step final : public StepBase {
     x.nr = s_.nr;
     x.opt_z = opt_z_;
     x.gas_step = gas_step_;
-    x.wide = wide_xy_ ? 1 : 0;
+    x.tile = tile_xy_;
     const dim3 xg((s_.n_rot + xy_tb_ - 1) / xy_tb_, static_cast<unsigned>(s_.n_zr()));
     prof_.begin(stream_);
     if (!(use_v2_ && launch_xy2<T>(x, s_.n_zr(), stream_))) spo::xy_pass_kernel<T><<<xg, 256, xy_smem_, stream_>>>(x);
@@ -792,40 +808,47 @@ class Step final : public StepBase {
     return ms / reps;
   }
 
-  // Chooses, per kinetic pass, between the narrow (16 lanes) and wide (32 lanes) tiles of the register
-  // kernels by timing both on the zero wave packet the handle starts with (a kinetic pass maps zero to
-  // zero, so the state is unchanged). Both tiles compute every line with the same operations in the
-  // same order: the choice changes the speed, never the result.
-  // SPO_B200_TILES=narrow|wide fixes the choice; SPO_B200_AUTOTUNE=0 keeps the narrow tiles.
+  // Chooses, per kinetic pass, the tile width (8, 16 or 32 batch lanes per block) of the register kernels
+  // with more than 8 sub-rows per line, by timing each on the zero wave packet the handle starts with
+  // (a kinetic pass maps zero to zero, so the state is unchanged). All widths compute every line with the
+  // same operations in the same order: the choice changes the speed, never the result.
+  // SPO_B200_TILES=8|16|32 fixes the choice; SPO_B200_AUTOTUNE=0 keeps the default (16).
   void autotune() {
-    wide_z_ = wide_r_ = wide_xy_ = false;
-    tiles_source_ = "narrow";
+    tile_z_ = tile_r_ = tile_xy_ = 0;
+    tiles_source_ = "default";
     if (!use_v2_) return;
     if (const char* env = std::getenv("SPO_B200_TILES")) {
       const std::string t(env);
-      require(t == "narrow" || t == "wide", "SPO_B200_TILES must be narrow or wide");
-      wide_z_ = wide_r_ = wide_xy_ = t == "wide";
-      tiles_source_ = t + "(fixed)";
+      require(t == "8" || t == "16" || t == "32", "SPO_B200_TILES must be 8, 16 or 32");
+      tile_z_ = tile_r_ = tile_xy_ = std::stoi(t);
+      tiles_source_ = "fixed";
       return;
     }
     if (const char* env = std::getenv("SPO_B200_AUTOTUNE"))
       if (std::string(env) == "0") return;
     constexpr int reps = 3;
     const double b = 0.0;
-    auto choose = [&](bool& flag, auto&& run) {
-      flag = false;
-      const float narrow = time_launches(run, reps);
-      flag = true;
-      const float wide = time_launches(run, reps);
-      flag = wide < 0.98f * narrow;  // keep the narrow tile unless the wide one is clearly faster
+    auto choose = [&](int& tile, auto&& run) {
+      int best = 16;
+      tile = 16;
+      float best_ms = time_launches(run, reps);
+      for (const int t : {8, 32}) {
+        tile = t;
+        const float ms = time_launches(run, reps);
+        if (ms < 0.98f * best_ms) {  // another width only when clearly faster
+          best = t;
+          best_ms = ms;
+        }
+      }
+      tile = best;
     };
     const bool was_on = prof_.on();
     prof_.enable(false);
-    if (axis2_supported(s_.nz))
-      choose(wide_z_, [&] { axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zk_full_, wide_z_); });
-    if (axis2_supported(s_.nr))
-      choose(wide_r_, [&] { axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rk_full_, wide_r_); });
-    if (s_.nx == s_.ny && xy2_supported(s_.nx)) choose(wide_xy_, [&] { kinetic_xy(false, false); });
+    if (axis2_supported(s_.nz) && axis2_has_tiles(s_.nz))
+      choose(tile_z_, [&] { axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zk_full_, tile_z_); });
+    if (axis2_supported(s_.nr) && axis2_has_tiles(s_.nr))
+      choose(tile_r_, [&] { axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rk_full_, tile_r_); });
+    if (s_.nx == s_.ny && xy2_supported(s_.nx) && s_.nx > 8) choose(tile_xy_, [&] { kinetic_xy(false, false); });
     prof_.enable(was_on);
     launches_ = 0;
     tiles_source_ = "autotuned";
@@ -1206,8 +1229,11 @@ class Step final : public StepBase {
       for (int b = 0; b < s.n_blocks; ++b)
         for (int j = 0; j < size[b]; ++j) {
           irot_slot[first[b] + j] = slot[b];
-          for (int t = 0; t < s.nt; ++t)
-            rows[static_cast<std::size_t>(first[b] + j) * (s.nt + 4) + t] = legendre[offset[b] + t * size[b] + j];
+          for (int t = 0; t < s.nt; ++t) {
+            const int quads = s.nt / 4;  // theta t at the position where the forward tiles read it
+            const int pos = (t % quads) * 4 + t / quads;
+            rows[static_cast<std::size_t>(first[b] + j) * (s.nt + 4) + pos] = legendre[offset[b] + t * size[b] + j];
+          }
         }
       pot4_smem_ = spo::pot4_smem<T>(s.n_rot, s.nphi, s.nt, cb, len);
       if (pot4_smem_ <= static_cast<std::size_t>(smem_optin)) {
@@ -1321,8 +1347,8 @@ class Step final : public StepBase {
   std::size_t pot4_smem_ = 0;
   int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4
   std::string pot_source_ = "default";
-  bool wide_z_ = false, wide_r_ = false, wide_xy_ = false;
-  std::string tiles_source_ = "narrow";
+  int tile_z_ = 0, tile_r_ = 0, tile_xy_ = 0;  // batch lanes per block of the register kinetic kernels (0: default)
+  std::string tiles_source_ = "default";
   // Asymptotic analysis (FP64).
   std::vector<cplx> shift_host_;
   spo_analysis_desc an_{};

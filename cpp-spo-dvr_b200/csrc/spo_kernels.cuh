@@ -258,7 +258,8 @@ struct XyArgs {
   int nr;
   const T* opt_z;          // nz
   const Vec<T>* gas_step;  // (ir, irot): opt_r rot gas rot
-  int wide;                // launch choice of the register-DFT xy kernel: 32 rotational states per block
+  int tile;                // launch choice of the register-DFT xy kernel: rotational states per block
+                           // (8, 16 or 32; 0: the default) for grids of more than 8 points per axis
 };
 
 template <typename T>

@@ -4,12 +4,13 @@
 // One block per SM slot loops over work items (a (Z, r) point and a chunk of CB (x, y) columns),
 // NT * CB = 128 threads. The angular matrix M_m[theta, J] = sqrt(w_theta / nphi) P_J^m(theta) is
 // staged in shared memory once per block, one row per rotational state irot (its block m, its J),
-// theta contiguous and the row padded to NT + 4 values, so that the 16-byte loads of consecutive
-// rows fall on distinct bank groups. Per item:
+// the row padded to NT + 4 values, so that the 16-byte loads of consecutive rows fall on distinct
+// bank groups; within a row theta is stored in the order in which the forward tiles take it. Per item:
 //   load:    F[irot][c] = opt_Z before(ir, irot) psi(c, irot), plus rot(dt/2) e0(c) chi(ir, iz) in the
 //            initial channel (potential_operator.cpp:116-123);
 //   forward: X[p][theta][c] = sum_J M_m[theta, J] F[first_m + J][c] for the slot p of every mJ block m,
-//            each thread a tile of 4 theta x 2 columns (16 FMAs per two 16-byte loads). The slots are
+//            each thread a tile of 4 theta (strided by NT / 4) x 2 columns (16 FMAs per two 16-byte
+//            loads, conflict-free stores). The slots are
 //            dealt to half-warps in +m / -m pairs (equal trip counts within a warp), balanced over the
 //            warps by their J counts; slots without basis functions are written as zeros;
 //   phi:     thread (theta, c) takes its line of NPHI slots into registers: DFT (sign +1), times
@@ -17,8 +18,8 @@
 //   back:    thread irot sums over theta for all CB columns (one matrix element reused CB times, the
 //            CB slot values of one theta read as 16-byte vectors), times rot(dt/2), stores psi;
 //   projection onto the specular grid: projection_finalize_kernel, after this kernel.
-// Every column goes through the same operations in the same order as in potential3_kernel, so the two
-// kernels give the same wave packet bit for bit.
+// The back sums take theta in the tiles' order (not ascending), so the result agrees with the other
+// potential kernels to rounding.
 #pragma once
 
 #include "spo_regfft.cuh"
@@ -28,7 +29,8 @@ namespace spo {
 template <typename T>
 struct Pot4Args {
   PotArgs<T> p;              // pointers and sizes shared with the other potential kernels
-  const T* leg_rows;         // n_rot rows of NT + 4: M_m[theta, J] of irot = first_m + J, theta contiguous
+  const T* leg_rows;         // n_rot rows of NT + 4: M_m[theta, J] of irot = first_m + J, theta at position
+                             // (theta % (NT / 4)) * 4 + theta / (NT / 4)
   const int* slot_first;     // per phi slot: first irot of its mJ block
   const int* slot_nj;        // per phi slot: J count (0: no basis functions)
   const int* irot_slot;      // per irot: its phi slot
@@ -64,29 +66,37 @@ SPO_HD void st2c(double2* p, double2 a, double2 b) {
   p[1] = b;
 }
 
-// Shared memory of potential4_kernel: F (n_rot CB), X (NPHI NT CB), the matrix rows (n_rot (NT + 4)),
+// X holds one block of NT * CB values per phi slot, each followed by 16 bytes of padding: the back sums
+// of a warp read the blocks of two or three slots at once, which then start on different banks.
+template <typename T>
+constexpr int pot4_slot_stride(int nt, int cb) {
+  return nt * cb + static_cast<int>(16 / sizeof(Vec<T>));
+}
+
+// Shared memory of potential4_kernel: F (n_rot CB), X (NPHI padded slot blocks), the matrix rows (n_rot (NT + 4)),
 // irot -> slot (n_rot ints), the schedule (8 sched_len ints).
 template <typename T>
 constexpr std::size_t pot4_smem(int n_rot, int nphi, int nt, int cb, int sched_len) {
-  return sizeof(Vec<T>) * (static_cast<std::size_t>(n_rot) * cb + static_cast<std::size_t>(nphi) * nt * cb) +
+  return sizeof(Vec<T>) * (static_cast<std::size_t>(n_rot) * cb + static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb)) +
          sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) + sizeof(int) * (static_cast<std::size_t>(n_rot) + 8 * sched_len);
 }
 
 template <typename T, int NPHI, int NT, int CB>
-__global__ void __launch_bounds__(NT * CB) potential4_kernel(Pot4Args<T> g) {
+__global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_kernel(Pot4Args<T> g) {
   using V = Vec<T>;
   static_assert(NT * CB == 128 && NT % 4 == 0 && CB % 2 == 0, "tile shape");
   constexpr int NTH = NT * CB;
   constexpr int LDL = NT + 4;
-  constexpr int QUADS = NT / 4;       // theta quads per slot tile
+  constexpr int QUADS = NT / 4;       // theta sets of 4 per slot tile
   constexpr int PAIRS = CB / 2;       // column pairs per slot tile
   static_assert(QUADS * PAIRS == 16, "a slot tile is one half-warp");
+  constexpr int SS = pot4_slot_stride<T>(NT, CB);  // X values per slot block
   const PotArgs<T>& a = g.p;
   const int n_rot = a.n_rot;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* F = reinterpret_cast<V*>(smem_raw);                   // [irot][c]
-  V* X = F + n_rot * CB;                                   // [p][theta][c]
-  T* L = reinterpret_cast<T*>(X + NPHI * NT * CB);         // [irot][theta], rows of LDL
+  V* X = F + n_rot * CB;                                   // [p][theta][c], slot blocks of SS values
+  T* L = reinterpret_cast<T*>(X + NPHI * SS);              // [irot][position of theta], rows of LDL
   int* irot_slot = reinterpret_cast<int*>(L + n_rot * LDL);
   int* sched = irot_slot + n_rot;                          // [group][k]
   const int tid = threadIdx.x;
@@ -94,46 +104,77 @@ __global__ void __launch_bounds__(NT * CB) potential4_kernel(Pot4Args<T> g) {
   for (int k = tid; k < n_rot; k += NTH) irot_slot[k] = g.irot_slot[k];
   for (int k = tid; k < 8 * g.sched_len; k += NTH) sched[k] = g.fwd_sched[k];
   __syncthreads();
-  // forward tile of this thread: theta quad fq, column pair fc, half-warp group fg
-  const int fq = tid % QUADS;
-  const int fc = (tid / QUADS) % PAIRS;
+  // Forward tile of this thread: column pair fc (fastest), theta set fq = {fq + QUADS q, q < 4} (the
+  // matrix row holds these four at positions 4 fq .. 4 fq + 3), half-warp group fg. The 8 threads of a
+  // 16-byte store phase then write two adjacent theta rows of X: distinct banks.
+  const int fc = tid % PAIRS;
+  const int fq = (tid / PAIRS) % QUADS;
   const int fg = tid / 16;
   // phi line of this thread
   const int line_c = tid % CB;
   const int line_t = tid / CB;
   const int i0 = a.initial_channel;
+  // Load tasks: task k = (irot k / PAIRS, column pair k % PAIRS); a warp's 32 tasks store 512
+  // contiguous bytes of F.
+  const int n_tasks = n_rot * PAIRS;
+  auto load_task = [&](long long col_base, int ncol, int k, V& v0, V& v1) {
+    const int irot = k / PAIRS;
+    const int c = 2 * (k - irot * PAIRS);
+    v0 = c < ncol ? a.psi[(col_base + c) * n_rot + irot] : cmake<V>(0, 0);
+    v1 = c + 1 < ncol ? a.psi[(col_base + c + 1) * n_rot + irot] : cmake<V>(0, 0);
+  };
+  auto item_columns = [&](long long item, int& izr, int& c0, int& ncol, long long& col_base) {
+    izr = static_cast<int>(item / g.chunks);
+    const int chunk = static_cast<int>(item - static_cast<long long>(izr) * g.chunks);
+    c0 = chunk * CB;
+    ncol = min(CB, a.n_xy - c0);
+    col_base = static_cast<long long>(izr) * a.n_xy + c0;
+  };
 
   for (long long item = blockIdx.x; item < g.n_items; item += gridDim.x) {
-    const int izr = static_cast<int>(item / g.chunks);
-    const int chunk = static_cast<int>(item - static_cast<long long>(izr) * g.chunks);
+    int izr, c0, ncol;
+    long long col_base;
+    item_columns(item, izr, c0, ncol, col_base);
     const int ir = izr % a.nr;
     const int iz = izr / a.nr;
-    const int c0 = chunk * CB;
-    const int ncol = min(CB, a.n_xy - c0);
-    const long long col_base = static_cast<long long>(izr) * a.n_xy + c0;
     const T oz = a.opt_z[iz];
     // No barrier here: F is read only by the forward phase, which ended before the previous item's
     // second barrier; X is rewritten only after this item's first barrier.
 
-    // ---- load
-    for (int irot = tid; irot < n_rot; irot += NTH) {
+    // ---- load: absorbers, rot(dt/2), the specular wave into the initial channel
+    auto store_task = [&](int k, V v0, V v1) {
+      const int irot = k / PAIRS;
+      const int c = 2 * (k - irot * PAIRS);
       const V b = a.before[ir * n_rot + irot];
-      V v[CB];
-#pragma unroll
-      for (int c = 0; c < CB; ++c) {
-        v[c] = c < ncol ? cscale(cmul(b, a.psi[(col_base + c) * n_rot + irot]), oz) : cmake<V>(0, 0);
-      }
+      v0 = c < ncol ? cscale(cmul(b, v0), oz) : cmake<V>(0, 0);
+      v1 = c + 1 < ncol ? cscale(cmul(b, v1), oz) : cmake<V>(0, 0);
       if (irot == i0) {
         const V incoming = a.chi[izr];
         const V rot_i0 = a.rot_half[ir * n_rot + i0];
+        if (c < ncol) v0 = cadd(v0, cmul(rot_i0, cmul(a.sp2sc[c0 + c], incoming)));
+        if (c + 1 < ncol) v1 = cadd(v1, cmul(rot_i0, cmul(a.sp2sc[c0 + c + 1], incoming)));
+      }
+      st2c(F + irot * CB + c, v0, v1);
+    };
+    // FP64: batches of 4 tasks, all their loads issued before the first is used (in the mixed form the
+    // registers are taken by the exp(i A) line of the phase after next: batching there spills).
+    constexpr int LB = sizeof(T) == 4 ? 1 : 4;
+    for (int k0 = tid; k0 < n_tasks; k0 += NTH * LB) {
+      V v0[LB], v1[LB];
 #pragma unroll
-        for (int c = 0; c < CB; ++c)
-          if (c < ncol) v[c] = cadd(v[c], cmul(rot_i0, cmul(a.sp2sc[c0 + c], incoming)));
+      for (int i = 0; i < LB; ++i) {
+        const int k = k0 + NTH * i;
+        if (k < n_tasks) load_task(col_base, ncol, k, v0[i], v1[i]);
       }
 #pragma unroll
-      for (int c = 0; c < CB; c += 2) st2c(F + irot * CB + c, v[c], v[c + 1]);
+      for (int i = 0; i < LB; ++i) {
+        const int k = k0 + NTH * i;
+        if (k < n_tasks) store_task(k, v0[i], v1[i]);
+      }
     }
     __syncthreads();
+
+    const bool has_line = line_c < ncol;
 
     // ---- forward theta contraction
     for (int k = 0; k < g.sched_len; ++k) {
@@ -145,7 +186,7 @@ __global__ void __launch_bounds__(NT * CB) potential4_kernel(Pot4Args<T> g) {
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[q][e] = 0;
+        for (int r = 0; r < 4; ++r) acc[q][r] = 0;
       const T* lp = L + first * LDL + 4 * fq;
       const V* fp = F + first * CB + 2 * fc;
       for (int j = 0; j < nj; ++j) {
@@ -163,50 +204,63 @@ __global__ void __launch_bounds__(NT * CB) potential4_kernel(Pot4Args<T> g) {
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        st2c(X + (slot * NT + 4 * fq + q) * CB + 2 * fc, cmake<V>(acc[q][0], acc[q][1]), cmake<V>(acc[q][2], acc[q][3]));
+        st2c(X + slot * SS + (fq + QUADS * q) * CB + 2 * fc, cmake<V>(acc[q][0], acc[q][1]),
+             cmake<V>(acc[q][2], acc[q][3]));
+    }
+    // Mixed form: exp(i A) of this thread's phi line (no symmetry maps), requested before the barrier,
+    // so that the loads overlap the other threads' last forward tiles (FP64 has no registers to spare).
+    constexpr bool EARLY_EXP = sizeof(T) == 4;
+    V e[EARLY_EXP ? NPHI : 1];
+    const bool direct = EARLY_EXP && g.identity_maps && has_line;
+    if (direct) {
+      const V* ep = a.expia + ((static_cast<long long>(izr) * a.n_rep + c0 + line_c) * NT + line_t) * NPHI;
+      static_for<0, NPHI / 2>([&](auto h) { ld2c(ep + 2 * SPO_CV(h), e[2 * SPO_CV(h)], e[2 * SPO_CV(h) + 1]); });
     }
     __syncthreads();
 
     // ---- phi transform, exp(i A), inverse phi transform, one line per thread
-    if (line_c < ncol) {
+    if (has_line) {
       const int ixy = c0 + line_c;
       V x[NPHI];
-      static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = X[(SPO_CV(p) * NT + line_t) * CB + line_c]; });
+      V* xl = X + line_t * CB + line_c;
+      static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
       rdft<NPHI, +1>(x);
-      if (g.identity_maps) {
-        const V* e = a.expia + ((static_cast<long long>(izr) * a.n_rep + ixy) * NT + line_t) * NPHI;
+      if (direct) {
+        if constexpr (EARLY_EXP) static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(e[SPO_CV(p)], x[SPO_CV(p)]); });
+      } else if (g.identity_maps) {
+        const V* ep = a.expia + ((static_cast<long long>(izr) * a.n_rep + ixy) * NT + line_t) * NPHI;
         static_for<0, NPHI / 2>([&](auto h) {
           constexpr int P = 2 * SPO_CV(h);
           V e0, e1;
-          ld2c(e + P, e0, e1);
+          ld2c(ep + P, e0, e1);
           x[P] = cmul(e0, x[P]);
           x[P + 1] = cmul(e1, x[P + 1]);
         });
       } else {
-        const V* e = a.expia + ((static_cast<long long>(izr) * a.n_rep + __ldg(a.rep_of + ixy)) * NT + line_t) * NPHI;
+        const V* ep = a.expia + ((static_cast<long long>(izr) * a.n_rep + __ldg(a.rep_of + ixy)) * NT + line_t) * NPHI;
         const int* map = a.phi_map + ixy * NPHI;
-        static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(__ldg(e + __ldg(map + SPO_CV(p))), x[SPO_CV(p)]); });
+        static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(__ldg(ep + __ldg(map + SPO_CV(p))), x[SPO_CV(p)]); });
       }
       rdft<NPHI, -1>(x);
-      static_for<0, NPHI>([&](auto p) { X[(SPO_CV(p) * NT + line_t) * CB + line_c] = x[SPO_CV(p)]; });
+      static_for<0, NPHI>([&](auto p) { xl[SPO_CV(p) * SS] = x[SPO_CV(p)]; });
     }
     __syncthreads();
 
-    // ---- transposed theta contraction, rot(dt/2), store, projection share
+    // ---- transposed theta contraction, rot(dt/2), store
     for (int irot = tid; irot < n_rot; irot += NTH) {
       const int slot = irot_slot[irot];
       T acc[CB][2];
 #pragma unroll
       for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = 0;
       const T* lrow = L + irot * LDL;
-      const V* ys = X + slot * NT * CB;
+      const V* ys = X + slot * SS;
 #pragma unroll 1
-      for (int tq = 0; tq < NT; tq += 4) {
+      for (int kq = 0; kq < QUADS; ++kq) {
         T l[4];
-        ld4(lrow + tq, l);
+        ld4(lrow + 4 * kq, l);  // theta kq + QUADS q, q < 4
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const V* y = ys + (tq + q) * CB;
+          const V* y = ys + (kq + QUADS * q) * CB;
 #pragma unroll
           for (int c = 0; c < CB; c += 2) {
             V y0, y1;

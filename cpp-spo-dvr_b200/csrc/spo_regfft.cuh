@@ -199,7 +199,8 @@ struct Axis2Args {
   long long inner;
   const Vec<T>* factor;  // N values, by k
   const Vec<T>* tw;      // N values: exp(-2 pi i j / N)
-  int wide;              // launch choice: 32 batch lanes per block where 16 is the default
+  int tile;              // launch choice: batch lanes per block (8, 16 or 32; 0: the default) for lines of
+                         // more than 8 sub-rows
 };
 
 // Dynamic shared memory: (N TB + 2 N) values (axis2_smem).

@@ -13,7 +13,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libspo_b200.so")
+# The library built in-tree; SPO_B200_LIBRARY names another build of it (e.g. one compiled with other
+# tuning macros).
+LIB_PATH = os.environ.get("SPO_B200_LIBRARY") or os.path.join(os.path.dirname(_HERE), "lib", "libspo_b200.so")
 
 SPO_OK, SPO_ERR_INVALID, SPO_ERR_OOM, SPO_ERR_DEVICE, SPO_ERR_TIMEOUT, SPO_ERR_STATE = range(6)
 STATUS_NAMES = {0: "SPO_OK", 1: "SPO_ERR_INVALID", 2: "SPO_ERR_OOM", 3: "SPO_ERR_DEVICE",

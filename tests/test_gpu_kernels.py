@@ -12,9 +12,9 @@ contractions). v3 and v4 apply the same operations in the same order to every co
 projection to a second kernel; they agree to rounding (not bitwise: the compiler may contract the
 products of a complex multiply into FMAs differently in each kernel).
 
-The narrow and wide tiles of the register kernels compute every line with the same operations in the
-same order, so the two give bitwise equal wave packets; the autotuner's choice between them can
-change the speed only.
+The tile widths of the register kernels (8, 16 or 32 batch lanes per block) compute every line with
+the same operations in the same order, so they give bitwise equal wave packets; the autotuner's
+choice between them can change the speed only.
 """
 
 import os
@@ -87,23 +87,24 @@ def test_register_kernels_match_general_kernels(shape, precision, kernels):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_narrow_and_wide_tiles_are_bitwise_equal(precision):
+def test_tile_widths_are_bitwise_equal(precision):
     from spo_b200 import workload
-    # Z 128 = 8 x 16 and (x, y) 16 x 16: the lengths whose kernels have both tiles
+    # Z 128 = 8 x 16 and (x, y) 16 x 16: the lengths whose kernels have 8, 16 and 32 lane tiles
     case = workload.config_case({"nz": 128, "nr": 24, "nx": 16, "ny": 16, "j_max": 3, "mj_max": 3,
                                  "nz_specular": 256, "nz_potential": 40})
     rng = np.random.default_rng(9)
     psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
     chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
     out = []
-    for tiles in ("narrow", "wide"):
+    for tiles in ("8", "16", "32"):
         be = make(case, "v3", precision, tiles)
-        assert tiles in be.describe(), be.describe()
+        assert f"z=axis2<128,tb{tiles}>" in be.describe() and f"xy=xy2<16,tb{tiles}>" in be.describe(), be.describe()
         be.read_wave_packet(psi0, chi0)
         be.propagate_analysis_step()
         out.append(be.wave_packet_on_host())
         be.close()
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for k in (1, 2):
+        assert np.array_equal(out[0][0], out[k][0]) and np.array_equal(out[0][1], out[k][1]), k
 
 
 @pytest.mark.parametrize("j_max", [15, 7, 3])
