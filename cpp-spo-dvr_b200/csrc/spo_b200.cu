@@ -163,6 +163,13 @@ bool launch_axis2_tb(const spo::Axis2Args<T>& a, long long outer, cudaStream_t s
   const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(N) * TB + 2 * N);
   static unsigned long long configured = 0;
   allow_smem(spo::axis2_kernel<T, N1, N2, TB>, smem, configured, "axis2 smem");
+  if (a.window > 0) {  // lane windows: groups x ceil(window / TB) blocks
+    spo::Axis2Args<T> w = a;
+    w.blocks_per_group = static_cast<int>((a.window + TB - 1) / TB);
+    const dim3 grid(static_cast<unsigned>(a.groups * w.blocks_per_group), static_cast<unsigned>(outer));
+    spo::axis2_kernel<T, N1, N2, TB><<<grid, TB * NS, smem, stream>>>(w);
+    return true;
+  }
   const dim3 grid(static_cast<unsigned>((a.inner + TB - 1) / TB), static_cast<unsigned>(outer));
   spo::axis2_kernel<T, N1, N2, TB><<<grid, TB * NS, smem, stream>>>(a);
   return true;
@@ -503,7 +510,7 @@ class Step final : public StepBase {
       out += " potential=potential2<nphi=" + std::to_string(s_.nphi) + ",cb=" + std::to_string(pot2_cb_) + ">";
     else
       out += " potential=potential(general)";
-    out += " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
+    out += " zr_window=" + std::to_string(zr_window_) + " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
     return out;
   }
 
@@ -699,11 +706,45 @@ class Step final : public StepBase {
          kinetic_only ? nullptr : spec_w_);
   }
 
-  // T_Z and T_r of the scattering wave.
+  // T_Z and T_r of the scattering wave. With zr_window_ > 0 the two passes run window by window over the
+  // (x, y, irot) lanes, Z then r for each window, so that a window written by the Z pass is still in L2
+  // when the r pass reads it (nz nr window values per window).
   void kinetic_zr(bool half) {
     const double b = 2.0 * sizeof(V) * s_.n_psi();
-    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, tile_z_);
-    axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, tile_r_);
+    const V* zf = half ? zk_half_ : zk_full_;
+    const V* rf = half ? rk_half_ : rk_full_;
+    if (zr_window_ == 0) {
+      axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zf, tile_z_);
+      axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rf, tile_r_);
+      return;
+    }
+    const long long lanes = s_.n_xy() * s_.n_rot;  // contiguous values per (Z, r) point
+    for (long long l0 = 0; l0 < lanes; l0 += zr_window_) {
+      const long long w = std::min<long long>(zr_window_, lanes - l0);
+      const double bw = b * static_cast<double>(w) / static_cast<double>(lanes);
+      spo::Axis2Args<T> z{psi_, 0, zf, tw_z_, tile_z_};
+      z.groups = s_.nr;  // lanes (ir, l0 + l): groups ir, lanes apart
+      z.group_stride = lanes;
+      z.lane_offset = l0;
+      z.window = w;
+      z.line_stride = static_cast<long long>(s_.nr) * lanes;
+      z.outer_stride = 0;
+      prof_.begin(stream_);
+      launch_axis2<T>(plan_z_.n, z, 1, stream_);
+      prof_.end(stream_, "kinetic_z", bw);
+      ++launches_;
+      spo::Axis2Args<T> r{psi_, 0, rf, tw_r_, tile_r_};
+      r.groups = 1;
+      r.group_stride = 0;
+      r.lane_offset = l0;
+      r.window = w;
+      r.line_stride = lanes;
+      r.outer_stride = static_cast<long long>(s_.nr) * lanes;  // block y = iz
+      prof_.begin(stream_);
+      launch_axis2<T>(plan_r_.n, r, s_.nz, stream_);
+      prof_.end(stream_, "kinetic_r", bw);
+      ++launches_;
+    }
   }
 
   // A kinetic axis pass over psi: the register-DFT kernel for its length when instantiated, else the
@@ -815,6 +856,7 @@ class Step final : public StepBase {
   // SPO_B200_TILES=8|16|32 fixes the choice; SPO_B200_AUTOTUNE=0 keeps the default (16).
   void autotune() {
     tile_z_ = tile_r_ = tile_xy_ = 0;
+    zr_window_ = 0;
     tiles_source_ = "default";
     if (!use_v2_) return;
     if (const char* env = std::getenv("SPO_B200_TILES")) {
@@ -822,8 +864,12 @@ class Step final : public StepBase {
       require(t == "8" || t == "16" || t == "32", "SPO_B200_TILES must be 8, 16 or 32");
       tile_z_ = tile_r_ = tile_xy_ = std::stoi(t);
       tiles_source_ = "fixed";
-      return;
     }
+    if (const char* env = std::getenv("SPO_B200_ZR_WINDOW")) {  // lanes per Z+r window (0: two full passes)
+      zr_window_ = std::max(0ll, std::stoll(env) / 32 * 32);
+      tiles_source_ = "fixed";
+    }
+    if (tiles_source_ == "fixed") return;
     if (const char* env = std::getenv("SPO_B200_AUTOTUNE"))
       if (std::string(env) == "0") return;
     constexpr int reps = 3;
@@ -849,6 +895,26 @@ class Step final : public StepBase {
     if (axis2_supported(s_.nr) && axis2_has_tiles(s_.nr))
       choose(tile_r_, [&] { axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rk_full_, tile_r_); });
     if (s_.nx == s_.ny && xy2_supported(s_.nx) && s_.nx > 8) choose(tile_xy_, [&] { kinetic_xy(false, false); });
+    // Z and r through L2: windows whose values (nz nr window) take about 24, 48 or 96 MB, against
+    // the two full passes.
+    zr_window_ = 0;
+    if (axis2_supported(s_.nz) && axis2_supported(s_.nr)) {
+      const long long lanes = s_.n_xy() * s_.n_rot;
+      float best_ms = time_launches([&] { kinetic_zr(false); }, reps);
+      long long best = 0;
+      for (const long long mb : {24ll, 48ll, 96ll}) {
+        long long w = (mb << 20) / (static_cast<long long>(s_.nz) * s_.nr * static_cast<long long>(sizeof(V)));
+        w = (w / 32) * 32;
+        if (w < 32 || w >= lanes) continue;
+        zr_window_ = w;
+        const float ms = time_launches([&] { kinetic_zr(false); }, reps);
+        if (ms < 0.98f * best_ms) {
+          best = w;
+          best_ms = ms;
+        }
+      }
+      zr_window_ = best;
+    }
     prof_.enable(was_on);
     launches_ = 0;
     tiles_source_ = "autotuned";
@@ -1348,6 +1414,7 @@ class Step final : public StepBase {
   int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4
   std::string pot_source_ = "default";
   int tile_z_ = 0, tile_r_ = 0, tile_xy_ = 0;  // batch lanes per block of the register kinetic kernels (0: default)
+  long long zr_window_ = 0;                     // lanes per Z+r window (0: two full passes)
   std::string tiles_source_ = "default";
   // Asymptotic analysis (FP64).
   std::vector<cplx> shift_host_;

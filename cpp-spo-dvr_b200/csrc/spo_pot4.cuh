@@ -2,10 +2,11 @@
 // contractions (src/propagation/potential_operator.cpp:84-135, angular_transform.cpp:54-114).
 //
 // One block per SM slot loops over work items (a (Z, r) point and a chunk of CB (x, y) columns),
-// NT * CB = 128 threads. The angular matrix M_m[theta, J] = sqrt(w_theta / nphi) P_J^m(theta) is
-// staged in shared memory once per block, one row per rotational state irot (its block m, its J),
-// the row padded to NT + 4 values, so that the 16-byte loads of consecutive rows fall on distinct
-// bank groups; within a row theta is stored in the order in which the forward tiles take it. Per item:
+// NT * CB = 128 threads. The angular matrix M_m[theta, J] = sqrt(w_theta / nphi) P_J^m(theta) has one
+// row per rotational state irot (its block m, its J), padded to NT + 4 values, so that the 16-byte
+// loads of consecutive rows fall on distinct bank groups; within a row theta is stored in the order in
+// which the forward tiles take it. The mixed form stages it in shared memory once per block, FP64 reads
+// it through L1 (pot4_matrix_shared). Per item:
 //   load:    F[irot][c] = opt_Z before(ir, irot) psi(c, irot), plus rot(dt/2) e0(c) chi(ir, iz) in the
 //            initial channel (potential_operator.cpp:116-123);
 //   forward: X[p][theta][c] = sum_J M_m[theta, J] F[first_m + J][c] for the slot p of every mJ block m,
@@ -73,12 +74,21 @@ constexpr int pot4_slot_stride(int nt, int cb) {
   return nt * cb + static_cast<int>(16 / sizeof(Vec<T>));
 }
 
-// Shared memory of potential4_kernel: F (n_rot CB), X (NPHI padded slot blocks), the matrix rows (n_rot (NT + 4)),
-// irot -> slot (n_rot ints), the schedule (8 sched_len ints).
+// Where the matrix rows live: shared memory in the mixed form (20 KB on config 2); in FP64 (40 KB) they
+// are read through L1 instead, so that two FP64 blocks fit per SM (10.3 against 12.7 ms per launch on
+// config 2, where the mixed form is fastest with them staged).
+template <typename T>
+constexpr bool pot4_matrix_shared() {
+  return sizeof(T) == 4;
+}
+
+// Shared memory of potential4_kernel: F (n_rot CB), X (NPHI padded slot blocks), the matrix rows
+// (n_rot (NT + 4), when staged), irot -> slot (n_rot ints), the schedule (8 sched_len ints).
 template <typename T>
 constexpr std::size_t pot4_smem(int n_rot, int nphi, int nt, int cb, int sched_len) {
   return sizeof(Vec<T>) * (static_cast<std::size_t>(n_rot) * cb + static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb)) +
-         sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) + sizeof(int) * (static_cast<std::size_t>(n_rot) + 8 * sched_len);
+         (pot4_matrix_shared<T>() ? sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) : 0) +
+         sizeof(int) * (static_cast<std::size_t>(n_rot) + 8 * sched_len);
 }
 
 template <typename T, int NPHI, int NT, int CB>
@@ -96,11 +106,14 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* F = reinterpret_cast<V*>(smem_raw);                   // [irot][c]
   V* X = F + n_rot * CB;                                   // [p][theta][c], slot blocks of SS values
-  T* L = reinterpret_cast<T*>(X + NPHI * SS);              // [irot][position of theta], rows of LDL
-  int* irot_slot = reinterpret_cast<int*>(L + n_rot * LDL);
+  constexpr bool L_SHARED = pot4_matrix_shared<T>();
+  T* Ls = reinterpret_cast<T*>(X + NPHI * SS);             // [irot][position of theta], rows of LDL
+  const T* L = L_SHARED ? Ls : g.leg_rows;
+  int* irot_slot = reinterpret_cast<int*>(Ls + (L_SHARED ? n_rot * LDL : 0));
   int* sched = irot_slot + n_rot;                          // [group][k]
   const int tid = threadIdx.x;
-  for (int k = tid; k < n_rot * LDL; k += NTH) L[k] = g.leg_rows[k];
+  if constexpr (L_SHARED)
+    for (int k = tid; k < n_rot * LDL; k += NTH) Ls[k] = g.leg_rows[k];
   for (int k = tid; k < n_rot; k += NTH) irot_slot[k] = g.irot_slot[k];
   for (int k = tid; k < 8 * g.sched_len; k += NTH) sched[k] = g.fwd_sched[k];
   __syncthreads();

@@ -201,6 +201,13 @@ struct Axis2Args {
   const Vec<T>* tw;      // N values: exp(-2 pi i j / N)
   int tile;              // launch choice: batch lanes per block (8, 16 or 32; 0: the default) for lines of
                          // more than 8 sub-rows
+  // Lane windows (all zero: every lane of [outer][N][inner]). Otherwise block x serves lanes
+  //   (x / blocks_per_group) * group_stride + lane_offset + (x % blocks_per_group) * TB + b,  b < TB,
+  // of which those with (x % blocks_per_group) * TB + b < window exist; the line's points are line_stride
+  // apart and block y's lines start y * outer_stride further.
+  int blocks_per_group;
+  long long group_stride, lane_offset, window, line_stride, outer_stride;
+  long long groups;  // host side: lane groups per line set (the launch has groups * blocks_per_group blocks)
 };
 
 // Dynamic shared memory: (N TB + 2 N) values (axis2_smem).
@@ -215,9 +222,20 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2_kernel(Axis2Args
   V* tw = f + N;
   const int b = threadIdx.x % TB;
   const int s = threadIdx.x / TB;
-  const long long i0 = static_cast<long long>(blockIdx.x) * TB;
-  const long long base = static_cast<long long>(blockIdx.y) * N * a.inner + i0 + b;
-  const bool lane_ok = i0 + b < a.inner;
+  long long base, stride;
+  bool lane_ok;
+  if (a.blocks_per_group == 0) {
+    const long long i0 = static_cast<long long>(blockIdx.x) * TB;
+    base = static_cast<long long>(blockIdx.y) * N * a.inner + i0 + b;
+    stride = a.inner;
+    lane_ok = i0 + b < a.inner;
+  } else {
+    const int grp = blockIdx.x / a.blocks_per_group;
+    const long long in_group = static_cast<long long>(blockIdx.x - grp * a.blocks_per_group) * TB + b;
+    base = static_cast<long long>(blockIdx.y) * a.outer_stride + grp * a.group_stride + a.lane_offset + in_group;
+    stride = a.line_stride;
+    lane_ok = in_group < a.window;
+  }
   for (int k = threadIdx.x; k < N; k += TB * NS) {
     f[k] = a.factor[k];
     tw[k] = a.tw[k];
@@ -228,7 +246,7 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2_kernel(Axis2Args
     const int n2 = s;
     V x[N1];
     static_for<0, N1>([&](auto n1) {
-      x[n1] = lane_ok ? a.data[base + static_cast<long long>(n2 + N2 * n1) * a.inner] : cmake<V>(0, 0);
+      x[n1] = lane_ok ? a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] : cmake<V>(0, 0);
     });
     rdft<N1, -1>(x);
     static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : cmul(x[k1], tw[n2 * k1]); });
@@ -251,7 +269,7 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2_kernel(Axis2Args
     V x[N1];
     static_for<0, N1>([&](auto k1) { x[k1] = Y[(n2 * N1 + k1) * TB + b]; });
     rdft<N1, +1>(x);
-    static_for<0, N1>([&](auto n1) { a.data[base + static_cast<long long>(n2 + N2 * n1) * a.inner] = x[n1]; });
+    static_for<0, N1>([&](auto n1) { a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] = x[n1]; });
   }
 }
 

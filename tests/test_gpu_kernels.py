@@ -128,3 +128,27 @@ def test_potential3_and_potential4_agree(j_max, precision):
         be.close()
     tol = 1e-13 if precision == "fp64" else 2e-6
     assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_zr_windows_are_bitwise_equal(precision, monkeypatch):
+    """T_Z and T_r run window by window over the (x, y, irot) lanes (Z then r per window, through L2):
+    the same lines with the same operations as the two full passes, so bitwise the same wave packet;
+    windows of 96 and 160 lanes (the last window of 160 is partial: 16 x 16 x 16 = 4096 lanes)."""
+    from spo_b200 import workload
+    case = workload.config_case({"nz": 128, "nr": 24, "nx": 16, "ny": 16, "j_max": 3, "mj_max": 3,
+                                 "nz_specular": 256, "nz_potential": 40})
+    rng = np.random.default_rng(13)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    out = []
+    for window in ("0", "96", "160"):
+        monkeypatch.setenv("SPO_B200_ZR_WINDOW", window)
+        be = make(case, "v4", precision)
+        assert f"zr_window={window}" in be.describe(), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    for k in (1, 2):
+        assert np.array_equal(out[0][0], out[k][0]) and np.array_equal(out[0][1], out[k][1]), k
