@@ -28,6 +28,7 @@
 #include "spo_kernels.cuh"
 #include "spo_regfft.cuh"
 #include "spo_pot4.cuh"
+#include "spo_pot5.cuh"
 
 namespace {
 
@@ -356,6 +357,21 @@ Pot4Kernel<T> pot4_kernel_for(int nphi, int nt) {
   return nullptr;
 }
 
+// The potential5 instantiation (mixed form only) for (nphi, ntheta), or null.
+template <typename T>
+using Pot5Kernel = void (*)(spo::Pot4Args<T>, int*);
+template <typename T>
+Pot5Kernel<T> pot5_kernel_for(int nphi, int nt) {
+  if constexpr (sizeof(T) != 4) {
+    return nullptr;
+  } else {
+    if (nt == 16 && nphi == 32) return spo::potential5_kernel<T, 32, 16, 8>;
+    if (nt == 8 && nphi == 16) return spo::potential5_kernel<T, 16, 8, 16>;
+    if (nt == 4 && nphi == 8) return spo::potential5_kernel<T, 8, 4, 32>;
+    return nullptr;
+  }
+}
+
 bool pot2_phi_supported(int nphi) {
   switch (nphi) {
     case 6: case 8: case 10: case 12: case 16: case 20: case 24: case 30: case 32: return true;
@@ -475,6 +491,18 @@ class Step final : public StepBase {
     enqueue_analysis_step();
     check_cuda(cudaStreamSynchronize(stream_), "propagate_analysis_step");
     prof_.resolve();
+    check_device_error();
+  }
+
+  // A kernel whose bounded wait gave up has set the device flag: report it (and clear it).
+  void check_device_error() {
+    if (!error_flag_) return;
+    int flag = 0;
+    check_cuda(cudaMemcpy(&flag, error_flag_, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+    if (flag) {
+      check_cuda(cudaMemset(error_flag_, 0, sizeof(int)), "error flag");
+      throw SpoError(SPO_ERR_TIMEOUT, "potential5: a bounded wait for an asynchronous copy gave up");
+    }
   }
 
   void enqueue_analysis_step() override {
@@ -500,7 +528,10 @@ class Step final : public StepBase {
     const bool xy2 = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx);
     out += std::string(" xy=") + (xy2 ? "xy2<" + std::to_string(s_.nx) + "," + lanes(tile_xy_, s_.nx > 8) + ">"
                                       : std::string("xy_pass(general)"));
-    if (pot_kind_ == 4)
+    if (pot_kind_ == 5)
+      out += " potential=potential5<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
+             ",cb=" + std::to_string(128 / s_.nt) + ",blocks=" + std::to_string(pot5_blocks_) + ">";
+    else if (pot_kind_ == 4)
       out += " potential=potential4<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
              ",cb=" + std::to_string(128 / s_.nt) + ",blocks=" + std::to_string(pot4_blocks_) + ">";
     else if (pot_kind_ == 3)
@@ -805,8 +836,10 @@ class Step final : public StepBase {
     prof_.begin(stream_);
     const double bytes = sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia()));
     const unsigned points = static_cast<unsigned>(s_.nzp) * s_.nr;
-    if (pot_kind_ == 3 || pot_kind_ == 4) {
-      if (pot_kind_ == 4) {
+    if (pot_kind_ >= 3) {
+      if (pot_kind_ == 5) {
+        pot5_kernel_<<<pot5_blocks_, 128, pot5_smem_, stream_>>>(pot4_args_, error_flag_);
+      } else if (pot_kind_ == 4) {
         pot4_kernel_<<<pot4_blocks_, 128, pot4_smem_, stream_>>>(pot4_args_);
       } else {
         const dim3 grid(static_cast<unsigned>(pot3_chunks_), points);
@@ -1302,6 +1335,24 @@ class Step final : public StepBase {
           }
         }
       pot4_smem_ = spo::pot4_smem<T>(s.n_rot, s.nphi, s.nt, cb, len);
+      // potential5: the same tables, the item data by bulk asynchronous copies (columns of n_rot values:
+      // 16-byte multiples when n_rot is even)
+      pot5_kernel_ = s.n_rot % 2 == 0 ? pot5_kernel_for<T>(s.nphi, s.nt) : nullptr;
+      pot5_smem_ = spo::pot5_smem<T>(s.n_rot, s.nphi, s.nt, cb, len);
+      if (pot5_kernel_ && pot5_smem_ <= static_cast<std::size_t>(smem_optin)) {
+        check_cuda(cudaFuncSetAttribute(pot5_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
+                   "potential5 smem");
+        int per_sm = 0, sms = 0;
+        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pot5_kernel_, 128, pot5_smem_),
+                   "potential5 occupancy");
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
+        pot5_blocks_per_sm_ = std::max(per_sm, 1);
+        pot5_sms_ = sms;
+        error_flag_ = dev<int>(1);
+        check_cuda(cudaMemset(error_flag_, 0, sizeof(int)), "error flag");
+      } else {
+        pot5_kernel_ = nullptr;
+      }
       if (pot4_smem_ <= static_cast<std::size_t>(smem_optin)) {
         check_cuda(cudaFuncSetAttribute(pot4_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
                    "potential4 smem");
@@ -1321,31 +1372,44 @@ class Step final : public StepBase {
         pot4_args_.identity_maps = pot2_.identity_maps;
         pot4_blocks_ = static_cast<int>(std::min<long long>(static_cast<long long>(std::max(per_sm, 1)) * sms,
                                                             std::max<long long>(pot4_args_.n_items, 1)));
+        pot5_blocks_ = static_cast<int>(std::min<long long>(static_cast<long long>(pot5_blocks_per_sm_) * pot5_sms_,
+                                                            std::max<long long>(pot4_args_.n_items, 1)));
       } else {
         pot4_kernel_ = nullptr;
+        pot5_kernel_ = nullptr;
       }
     }
-    if (pot3_cb_ > 0 || pot4_kernel_) {
+    if (pot3_cb_ > 0 || pot4_kernel_ || pot5_kernel_) {
       require(sizeof(V) * (nxy + 1) <= static_cast<std::size_t>(smem_optin), "nx*ny too large for the projection kernel");
       check_cuda(cudaFuncSetAttribute(spo::projection_finalize_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem_optin), "projection smem");
     }
     // The potential kernel is not chosen by timing: the kernels agree only to rounding (the compiler may
     // contract the products of a complex multiply into FMAs differently in each), and a timing choice
-    // could then differ between two runs of the same case. The order is fixed: 4, 3, 2, general.
+    // could then differ between two runs of the same case. The order is fixed: 4, 5, 3, 2, general.
     pot_kind_ = 1;
     if (use_v2_ && pot2_cb_ > 0) pot_kind_ = 2;
     if (use_v2_ && pot3_cb_ > 0) pot_kind_ = 3;
-    if (use_v2_ && pot4_kernel_) pot_kind_ = 4;
+    if (use_v2_ && pot5_kernel_) pot_kind_ = 5;
+    if (use_v2_ && pot4_kernel_) pot_kind_ = 4;  // faster than potential5 on configuration 3 (4.7 vs 5.0 ms)
     pot_source_ = "default";
     if (const char* env = std::getenv("SPO_B200_KERNELS")) {
       const std::string k(env);
-      require(k == "v1" || k == "v2" || k == "v3" || k == "v4", "SPO_B200_KERNELS must be v1, v2, v3 or v4");
+      require(k == "v1" || k == "v2" || k == "v3" || k == "v4" || k == "v5",
+              "SPO_B200_KERNELS must be v1, v2, v3, v4 or v5");
       use_v2_ = k != "v1";
       const int want = k[1] - '0';
       const bool have = want == 1 || (want == 2 && pot2_cb_ > 0) || (want == 3 && pot3_cb_ > 0) ||
-                        (want == 4 && pot4_kernel_ != nullptr);
-      pot_kind_ = have ? want : (use_v2_ && pot2_cb_ > 0 ? 2 : 1);
+                        (want == 4 && pot4_kernel_ != nullptr) || (want == 5 && pot5_kernel_ != nullptr);
+      // an unavailable kernel falls back to the best available one below it
+      const bool avail[6] = {false, true, pot2_cb_ > 0, pot3_cb_ > 0, pot4_kernel_ != nullptr, pot5_kernel_ != nullptr};
+      pot_kind_ = have ? want : 1;
+      if (!have)
+        for (int k = want - 1; k >= 2; --k)
+          if (use_v2_ && avail[k]) {
+            pot_kind_ = k;
+            break;
+          }
       pot_source_ = "fixed";
     }
     check_cuda(cudaStreamSynchronize(stream_), "set-up");
@@ -1411,7 +1475,11 @@ class Step final : public StepBase {
   spo::Pot4Args<T> pot4_args_{};
   int pot4_blocks_ = 0;
   std::size_t pot4_smem_ = 0;
-  int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4
+  Pot5Kernel<T> pot5_kernel_ = nullptr;
+  int pot5_blocks_ = 0, pot5_blocks_per_sm_ = 1, pot5_sms_ = 0;
+  std::size_t pot5_smem_ = 0;
+  int* error_flag_ = nullptr;  // set by a kernel whose bounded wait gave up
+  int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4, 5 potential5
   std::string pot_source_ = "default";
   int tile_z_ = 0, tile_r_ = 0, tile_xy_ = 0;  // batch lanes per block of the register kinetic kernels (0: default)
   long long zr_window_ = 0;                     // lanes per Z+r window (0: two full passes)

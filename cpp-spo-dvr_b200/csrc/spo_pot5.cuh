@@ -1,0 +1,340 @@
+// Potential step of the interaction region, mixed form, with the item data moved by bulk asynchronous
+// copies (src/propagation/potential_operator.cpp:84-135, angular_transform.cpp:54-114).
+//
+// potential4_kernel loads each item's wave packet and exp(i A) rows with ordinary per-thread loads when
+// it needs them; with 12 warps per SM that keeps too few bytes in flight (1.8 TB/s on configuration 3).
+// This kernel issues them one item ahead with cp.async.bulk (global -> shared, completion counted in
+// bytes on an mbarrier), so the copies of item k + 1 run while item k computes:
+//   - psi: the CB columns of the item (n_rot contiguous values each) into the F buffer, column c at
+//     F + c (n_rot + 2) (the 16-byte pad puts the columns on different banks); issued for item k + 1
+//     as soon as item k's forward sums have read F;
+//   - exp(i A): each thread's phi line (NPHI contiguous values of its column's representative) into its
+//     own row of E (rows of NPHI + 2 values: 16-byte loads of 8 consecutive rows on distinct banks);
+//     issued for item k + 1 when item k's phi phase is done.
+// Per item: wait for F; scale it in place (absorbers, rot(dt/2), the specular wave into the initial
+// channel); forward theta sums (potential4's tiles, F read column-major); wait for E; phi DFT, exp(i A),
+// inverse DFT; transposed theta sums, rot(dt/2), store. The matrix rows are staged in shared memory as
+// in potential4 (about 105 KB per block on configuration 3: two blocks per SM). The projection onto the
+// specular grid is projection_finalize_kernel's.
+//
+// Every wait on an mbarrier is bounded. A block whose wait gives up sets *error_flag, waits (bounded)
+// for the copies it has in flight and returns as a whole; the host reads the flag after the step.
+#pragma once
+
+#include <cstdint>
+
+#include "spo_pot4.cuh"
+
+namespace spo {
+
+namespace pot5 {
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Arrives on the barrier, announcing `bytes` more bytes of asynchronous copies for the current phase.
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 state;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 state, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .b64 state;\n\t"
+      "mbarrier.arrive.shared::cta.b64 state, [%0];\n\t}" ::"r"(smem_addr(bar))
+      : "memory");
+}
+
+// Waits for the phase with the given parity to complete; false after kWaitLimit polls.
+constexpr int kWaitLimit = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_addr(bar);
+  for (int i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Orders this thread's earlier shared-memory accesses before later asynchronous-proxy writes to them.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to this CTA's
+// shared memory, completing `bytes` on the barrier.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+}  // namespace pot5
+
+// Shared memory of potential5_kernel: 2 barriers (padded to 32 bytes), F (CB columns of n_rot + 2
+// values), E (NT CB rows of NPHI + 2 values), X (NPHI padded slot blocks), the matrix rows (n_rot rows
+// of NT + 4), irot -> slot (n_rot ints), the schedule (8 sched_len ints).
+template <typename T>
+constexpr std::size_t pot5_smem(int n_rot, int nphi, int nt, int cb, int sched_len) {
+  return 32 + sizeof(Vec<T>) * (static_cast<std::size_t>(cb) * (n_rot + 2) +
+                                static_cast<std::size_t>(nt) * cb * (nphi + 2) +
+                                static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb)) +
+         sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) +
+         sizeof(int) * (static_cast<std::size_t>(n_rot) + 8 * sched_len);
+}
+
+template <typename T, int NPHI, int NT, int CB>
+__global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, int* __restrict__ error_flag) {
+  using V = Vec<T>;
+  static_assert(sizeof(T) == 4, "the mixed form");
+  static_assert(NT * CB == 128 && NT % 4 == 0 && CB % 2 == 0, "tile shape");
+  constexpr int NTH = NT * CB;
+  constexpr int LDL = NT + 4;
+  constexpr int QUADS = NT / 4;
+  constexpr int PAIRS = CB / 2;
+  static_assert(QUADS * PAIRS == 16, "a slot tile is one half-warp");
+  constexpr int SS = pot4_slot_stride<T>(NT, CB);
+  constexpr int ERS = NPHI + 2;  // E row stride (values)
+  const PotArgs<T>& a = g.p;
+  const int n_rot = a.n_rot;
+  const int FCS = n_rot + 2;     // F column stride (values); n_rot is even
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // 0: F, 1: E
+  V* const F = reinterpret_cast<V*>(smem_raw + 32);  // [c][irot], columns of FCS values
+  V* E = F + CB * FCS;                     // [line][phi], line = thread
+  V* X = E + NTH * ERS;                    // [p][theta][c], slot blocks of SS values
+  T* L = reinterpret_cast<T*>(X + NPHI * SS);  // [irot][position of theta], rows of LDL
+  int* irot_slot = reinterpret_cast<int*>(L + n_rot * LDL);
+  int* sched = irot_slot + n_rot;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int k = 0; k < 2; ++k) pot5::mbar_init(bars + k, NTH);
+    pot5::mbar_init_fence();
+  }
+  for (int k = tid; k < n_rot * LDL; k += NTH) L[k] = g.leg_rows[k];
+  for (int k = tid; k < n_rot; k += NTH) irot_slot[k] = g.irot_slot[k];
+  for (int k = tid; k < 8 * g.sched_len; k += NTH) sched[k] = g.fwd_sched[k];
+  __syncthreads();
+
+  const int fc = tid % PAIRS;
+  const int fq = (tid / PAIRS) % QUADS;
+  const int fg = tid / 16;
+  const int line_c = tid % CB;
+  const int line_t = tid / CB;
+  const int i0 = a.initial_channel;
+  const uint32_t col_bytes = static_cast<uint32_t>(n_rot * sizeof(V));
+  constexpr uint32_t row_bytes = NPHI * sizeof(V);
+
+  auto item_columns = [&](long long item, int& izr, int& c0, int& ncol) {
+    izr = static_cast<int>(item / g.chunks);
+    c0 = static_cast<int>(item - static_cast<long long>(izr) * g.chunks) * CB;
+    ncol = min(CB, a.n_xy - c0);
+  };
+  // Every thread arrives on each barrier once per phase; the threads that copy announce their bytes.
+  auto issue_psi = [&](long long item) {
+    int izr, c0, ncol;
+    item_columns(item, izr, c0, ncol);
+    if (tid < ncol) {
+      pot5::fence_proxy_async();
+      pot5::mbar_arrive_tx(bars, col_bytes);
+      pot5::bulk_copy(F + tid * FCS, a.psi + (static_cast<long long>(izr) * a.n_xy + c0 + tid) * n_rot, col_bytes,
+                      bars);
+    } else {
+      pot5::mbar_arrive(bars);
+    }
+  };
+  auto issue_exp = [&](long long item) {
+    int izr, c0, ncol;
+    item_columns(item, izr, c0, ncol);
+    if (line_c < ncol) {
+      const int ixy = c0 + line_c;
+      const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
+      pot5::fence_proxy_async();
+      pot5::mbar_arrive_tx(bars + 1, row_bytes);
+      pot5::bulk_copy(E + tid * ERS, a.expia + ((static_cast<long long>(izr) * a.n_rep + rep) * NT + line_t) * NPHI,
+                      row_bytes, bars + 1);
+    } else {
+      pot5::mbar_arrive(bars + 1);
+    }
+  };
+  // A bounded wait by every thread; true (for the whole block) when one of them gave up.
+  auto wait_failed = [&](uint64_t* bar, uint32_t parity) {
+    const bool ok = pot5::mbar_wait(bar, parity);
+    return __syncthreads_or(!ok) != 0;
+  };
+  // Phase parities (bit 0: F, bit 1: E) and copies issued but not yet waited for (same bits).
+  uint32_t parity = 0, pending = 0;
+  auto give_up = [&]() {
+    if (tid == 0) atomicExch(error_flag, 1);
+    // bounded waits for this block's copies in flight, so that none lands after the block has left
+    for (int k = 0; k < 2; ++k)
+      if (pending >> k & 1u) pot5::mbar_wait(bars + k, parity >> k & 1u);
+  };
+
+  long long item = blockIdx.x;
+  if (item < g.n_items) {
+    issue_psi(item);
+    issue_exp(item);
+    pending = 3u;
+  }
+  for (; item < g.n_items; item += gridDim.x) {
+    int izr, c0, ncol;
+    item_columns(item, izr, c0, ncol);
+    const int ir = izr % a.nr;
+    const int iz = izr / a.nr;
+    const T oz = a.opt_z[iz];
+    const long long col_base = static_cast<long long>(izr) * a.n_xy + c0;
+
+    // ---- wait for the columns, scale them in place (absorbers, rot(dt/2), the specular wave)
+    if (wait_failed(bars, parity & 1u)) {
+      give_up();
+      return;
+    }
+    parity ^= 1u;
+    pending &= ~1u;
+    {
+      const V incoming = a.chi[izr];
+      const V rot_i0 = a.rot_half[ir * n_rot + i0];
+      for (int t = tid; t < CB * n_rot; t += NTH) {
+        const int c = t / n_rot;
+        const int irot = t - c * n_rot;
+        V v = cmake<V>(0, 0);
+        if (c < ncol) {
+          v = cscale(cmul(a.before[ir * n_rot + irot], F[c * FCS + irot]), oz);
+          if (irot == i0) v = cadd(v, cmul(rot_i0, cmul(a.sp2sc[c0 + c], incoming)));
+        }
+        F[c * FCS + irot] = v;
+      }
+    }
+    __syncthreads();
+    const long long next = item + gridDim.x;
+
+    // ---- forward theta contraction
+    for (int s = 0; s < g.sched_len; ++s) {
+      const int slot = sched[fg * g.sched_len + s];
+      if (slot < 0) continue;
+      const int nj = __ldg(g.slot_nj + slot);
+      const int first = nj > 0 ? __ldg(g.slot_first + slot) : 0;
+      T acc[4][4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[q][r] = 0;
+      const T* lp = L + first * LDL + 4 * fq;
+      const V* f0p = F + (2 * fc) * FCS + first;
+      const V* f1p = f0p + FCS;
+      for (int j = 0; j < nj; ++j) {
+        T l[4];
+        ld4(lp + j * LDL, l);
+        const V f0 = f0p[j];
+        const V f1 = f1p[j];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[q][0] += l[q] * f0.x;
+          acc[q][1] += l[q] * f0.y;
+          acc[q][2] += l[q] * f1.x;
+          acc[q][3] += l[q] * f1.y;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        st2c(X + slot * SS + (fq + QUADS * q) * CB + 2 * fc, cmake<V>(acc[q][0], acc[q][1]),
+             cmake<V>(acc[q][2], acc[q][3]));
+    }
+    __syncthreads();
+    // the next item's columns (every thread has finished reading F)
+    if (next < g.n_items) {
+      issue_psi(next);
+      pending |= 1u;
+    }
+
+    // ---- phi transform, exp(i A), inverse phi transform
+    if (wait_failed(bars + 1, parity >> 1 & 1u)) {
+      give_up();
+      return;
+    }
+    parity ^= 2u;
+    pending &= ~2u;
+    if (line_c < ncol) {
+      const int ixy = c0 + line_c;
+      V* xl = X + line_t * CB + line_c;
+      const V* el = E + tid * ERS;
+      V x[NPHI];
+      static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
+      rdft<NPHI, +1>(x);
+      if (g.identity_maps) {
+        static_for<0, NPHI / 2>([&](auto h) {
+          constexpr int P = 2 * SPO_CV(h);
+          V e0, e1;
+          ld2c(el + P, e0, e1);
+          x[P] = cmul(e0, x[P]);
+          x[P + 1] = cmul(e1, x[P + 1]);
+        });
+      } else {
+        const int* map = a.phi_map + ixy * NPHI;
+        static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(el[__ldg(map + SPO_CV(p))], x[SPO_CV(p)]); });
+      }
+      rdft<NPHI, -1>(x);
+      static_for<0, NPHI>([&](auto p) { xl[SPO_CV(p) * SS] = x[SPO_CV(p)]; });
+    }
+    __syncthreads();
+    // the next item's exp(i A) rows (every thread has read its row of this item)
+    if (next < g.n_items) {
+      issue_exp(next);
+      pending |= 2u;
+    }
+
+    // ---- transposed theta contraction, rot(dt/2), store
+    for (int irot = tid; irot < n_rot; irot += NTH) {
+      const int slot = irot_slot[irot];
+      T acc[CB][2];
+#pragma unroll
+      for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = 0;
+      const T* lrow = L + irot * LDL;
+      const V* ys = X + slot * SS;
+#pragma unroll 1
+      for (int kq = 0; kq < QUADS; ++kq) {
+        T l[4];
+        ld4(lrow + 4 * kq, l);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const V* y = ys + (kq + QUADS * q) * CB;
+#pragma unroll
+          for (int c = 0; c < CB; c += 2) {
+            V y0, y1;
+            ld2c(y + c, y0, y1);
+            acc[c][0] += l[q] * y0.x;
+            acc[c][1] += l[q] * y0.y;
+            acc[c + 1][0] += l[q] * y1.x;
+            acc[c + 1][1] += l[q] * y1.y;
+          }
+        }
+      }
+      const V rh = a.rot_half[ir * n_rot + irot];
+#pragma unroll
+      for (int c = 0; c < CB; ++c)
+        if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, cmake<V>(acc[c][0], acc[c][1]));
+    }
+  }
+}
+
+}  // namespace spo

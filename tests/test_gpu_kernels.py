@@ -56,7 +56,7 @@ def make(case, kernels, precision, tiles=None):
 
 @pytest.mark.parametrize("shape", list(SHAPES))
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("kernels", ["v2", "v3", "v4"])
+@pytest.mark.parametrize("kernels", ["v2", "v3", "v4", "v5"])
 def test_register_kernels_match_general_kernels(shape, precision, kernels):
     from spo_b200 import capi, workload
     case = workload.config_case(SHAPES[shape])
@@ -66,7 +66,10 @@ def test_register_kernels_match_general_kernels(shape, precision, kernels):
     tol_stage, tol_step = (1e-12, 1e-11) if precision == "fp64" else (2e-6, 2e-5)
     ref = make(case, "v1", precision)
     new = make(case, kernels, precision)
-    assert f"potential=potential{kernels[1]}" in new.describe(), new.describe()
+    if kernels == "v5" and precision == "fp64":  # potential5 is the mixed form's
+        assert "potential=potential4" in new.describe(), new.describe()
+    else:
+        assert f"potential=potential{kernels[1]}" in new.describe(), new.describe()
     for be in (ref, new):
         be.read_wave_packet(psi0, chi0)
     for stage in (capi.STAGE_ZR, capi.STAGE_XY, capi.STAGE_POTENTIAL):
@@ -152,3 +155,39 @@ def test_zr_windows_are_bitwise_equal(precision, monkeypatch):
         be.close()
     for k in (1, 2):
         assert np.array_equal(out[0][0], out[k][0]) and np.array_equal(out[0][1], out[k][1]), k
+
+
+@pytest.mark.parametrize("j_max", [15, 7, 3])
+def test_potential5_agrees_with_potential4(j_max):
+    """potential5 (bulk asynchronous copies, mixed form) against potential4 over an analysis step, on the
+    three instantiation families: the same sums in the same order except the FMA contraction choices
+    of each kernel, so they agree to FP32 rounding; then potential5 alone over four steps on a case
+    whose x-y grid is not a multiple of the column chunk (n_xy 36, 8 or 16 columns per chunk)."""
+    from spo_b200 import workload
+    case = workload.config_case({"nz": 32, "nr": 24, "nx": 8, "ny": 8, "j_max": j_max, "mj_max": j_max,
+                                 "nz_specular": 64, "nz_potential": 20})
+    rng = np.random.default_rng(5)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    out = []
+    for kernels in ("v4", "v5"):
+        be = make(case, kernels, "mixed")
+        assert f"potential=potential{kernels[1]}" in be.describe(), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    assert rel_err(out[1][0], out[0][0]) < 2e-6 and rel_err(out[1][1], out[0][1]) < 2e-6
+    ragged = workload.config_case({"nz": 24, "nr": 24, "nx": 6, "ny": 6, "j_max": j_max, "mj_max": j_max,
+                                   "nz_specular": 64, "nz_potential": 16})
+    psi0 = rng.standard_normal(ragged.psi_shape) + 1j * rng.standard_normal(ragged.psi_shape)
+    chi0 = rng.standard_normal(ragged.chi_shape) + 1j * rng.standard_normal(ragged.chi_shape)
+    res = []
+    for kernels in ("v1", "v5"):
+        be = make(ragged, kernels, "mixed")
+        be.read_wave_packet(psi0, chi0)
+        for _ in range(4):
+            be.propagate_analysis_step()
+        res.append(be.wave_packet_on_host())
+        be.close()
+    assert rel_l2(res[1][0], res[0][0]) < 2e-5 and rel_l2(res[1][1], res[0][1]) < 2e-5
