@@ -1386,12 +1386,12 @@ class Step final : public StepBase {
     }
     // The potential kernel is not chosen by timing: the kernels agree only to rounding (the compiler may
     // contract the products of a complex multiply into FMAs differently in each), and a timing choice
-    // could then differ between two runs of the same case. The order is fixed: 4, 5, 3, 2, general.
+    // could then differ between two runs of the same case. The order is fixed: 5, 4, 3, 2, general.
     pot_kind_ = 1;
     if (use_v2_ && pot2_cb_ > 0) pot_kind_ = 2;
     if (use_v2_ && pot3_cb_ > 0) pot_kind_ = 3;
+    if (use_v2_ && pot4_kernel_) pot_kind_ = 4;
     if (use_v2_ && pot5_kernel_) pot_kind_ = 5;
-    if (use_v2_ && pot4_kernel_) pot_kind_ = 4;  // faster than potential5 on configuration 3 (4.7 vs 5.0 ms)
     pot_source_ = "default";
     if (const char* env = std::getenv("SPO_B200_KERNELS")) {
       const std::string k(env);

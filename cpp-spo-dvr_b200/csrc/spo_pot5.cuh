@@ -211,18 +211,18 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     }
     parity ^= 1u;
     pending &= ~1u;
-    {
-      const V incoming = a.chi[izr];
-      const V rot_i0 = a.rot_half[ir * n_rot + i0];
-      for (int t = tid; t < CB * n_rot; t += NTH) {
-        const int c = t / n_rot;
-        const int irot = t - c * n_rot;
+    for (int irot = tid; irot < n_rot; irot += NTH) {
+      const V b = a.before[ir * n_rot + irot];
+#pragma unroll
+      for (int c = 0; c < CB; ++c) {
         V v = cmake<V>(0, 0);
-        if (c < ncol) {
-          v = cscale(cmul(a.before[ir * n_rot + irot], F[c * FCS + irot]), oz);
-          if (irot == i0) v = cadd(v, cmul(rot_i0, cmul(a.sp2sc[c0 + c], incoming)));
-        }
+        if (c < ncol) v = cscale(cmul(b, F[c * FCS + irot]), oz);
         F[c * FCS + irot] = v;
+      }
+      if (irot == i0) {
+        const V incoming = a.chi[izr];
+        const V rot_i0 = a.rot_half[ir * n_rot + i0];
+        for (int c = 0; c < ncol; ++c) F[c * FCS + i0] = cadd(F[c * FCS + i0], cmul(rot_i0, cmul(a.sp2sc[c0 + c], incoming)));
       }
     }
     __syncthreads();

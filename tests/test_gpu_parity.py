@@ -128,7 +128,7 @@ def test_errors_are_reported_not_thrown(ref_case):
 @pytest.mark.parametrize("name", TINY_CASES)
 def test_potential_kernels_match_oracle(ref_case, name, kernels, monkeypatch):
     """The potential step and two analysis steps with each chunked potential kernel forced (the default
-    takes the first available of potential4, potential5, potential3, ...). Cases whose angular grid the
+    takes the first available of potential5, potential4, potential3, ...). Cases whose angular grid the
     kernel does not cover are skipped; potential5 exists in the mixed form only (3e-5 over two steps)."""
     monkeypatch.setenv("SPO_B200_KERNELS", kernels)
     from spo_b200 import capi
