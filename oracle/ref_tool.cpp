@@ -201,6 +201,9 @@ void write_case(const fs::path& dir, const spodvr::BackendInput& in, const spodv
   m["j"] = j_of;
   m["mj"] = mj_of;
   std::ofstream(dir / "manifest.json") << m.dump(1);
+  // The angular DVR nodes (theta, phi), for features of the potential grid's points.
+  write_vec(dir / "grid_theta.f64", std::vector<double>(in.angular.thetas().begin(), in.angular.thetas().end()));
+  write_vec(dir / "grid_phi.f64", std::vector<double>(in.angular.phis().begin(), in.angular.phis().end()));
 
   auto c = [&](const char* name, const std::vector<cplx>& v) { write_vec(dir / (std::string(name) + ".c128"), v); };
   auto r = [&](const char* name, const std::vector<double>& v) { write_vec(dir / (std::string(name) + ".f64"), v); };

@@ -68,3 +68,29 @@ def test_null_handle_calls_are_refused():
     lib = capi.load_library()
     assert lib.spo_propagate_analysis_step(None) == capi.SPO_ERR_INVALID
     assert lib.spo_destroy(None) == capi.SPO_OK
+
+
+def mlp_header_functions():
+    text = open(os.path.join(ROOT, "include", "spo_mlp.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(spo_mlp_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_mlp_header_binding_and_library_agree():
+    """include/spo_mlp.h, the Python binding (spo_b200/mlp.py) and the library's symbols."""
+    _ensure_built()
+    from spo_b200 import capi, mlp
+    assert mlp_header_functions() == sorted(mlp._EXPORTS)
+    lib = capi.load_library()
+    for name in mlp_header_functions():
+        assert hasattr(lib, name), name
+
+
+def test_mlp_invalid_shapes_are_refused_without_a_device():
+    _ensure_built()
+    from spo_b200 import capi, mlp
+    lib = mlp._bind(capi.load_library())
+    h = ctypes.c_void_p()
+    assert lib.spo_mlp_create(65, 256, 4, 1, 0, ctypes.byref(h)) == capi.SPO_ERR_INVALID
+    assert "n_in" in lib.spo_mlp_last_error(None).decode()
+    assert lib.spo_mlp_create(8, 200, 4, 1, 0, ctypes.byref(h)) == capi.SPO_ERR_INVALID
+    assert "width" in lib.spo_mlp_last_error(None).decode()
