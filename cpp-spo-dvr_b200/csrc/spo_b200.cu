@@ -541,7 +541,7 @@ class Step final : public StepBase {
       out += " potential=potential2<nphi=" + std::to_string(s_.nphi) + ",cb=" + std::to_string(pot2_cb_) + ">";
     else
       out += " potential=potential(general)";
-    out += " zr_window=" + std::to_string(zr_window_) + " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
+    out += " zr_window=" + std::to_string(zr_window_) + " rxy_planes=" + std::to_string(rxy_planes_) + " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
     return out;
   }
 
@@ -721,9 +721,31 @@ class Step final : public StepBase {
   // ------------------------------------------------------------------ one sub-step
   void sub_step(bool half, bool kinetic_only) {
     specular(half, kinetic_only);
-    kinetic_zr(half);
-    kinetic_xy(half, !kinetic_only);  // the gas-phase potential step rides along
+    if (rxy_planes_ > 0) {
+      kinetic_rxy_slabs(half, !kinetic_only);
+    } else {
+      kinetic_zr(half);
+      kinetic_xy(half, !kinetic_only);  // the gas-phase potential step rides along
+    }
     if (!kinetic_only) interaction();
+  }
+
+  // T_Z over the whole wave packet, then T_r and T_xy slab by slab of rxy_planes_ Z planes (nr n_xy n_rot
+  // values each): T_r and T_xy of a point only involve its own Z plane, and a slab written by the r pass
+  // is still in L2 when the xy pass reads it.
+  void kinetic_rxy_slabs(bool half, bool with_gas) {
+    const double b = 2.0 * sizeof(V) * s_.n_psi();
+    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, tile_z_);
+    const long long plane = static_cast<long long>(s_.nr) * s_.n_xy() * s_.n_rot;
+    for (int iz0 = 0; iz0 < s_.nz; iz0 += rxy_planes_) {
+      const int g = std::min(rxy_planes_, s_.nz - iz0);
+      spo::Axis2Args<T> r{psi_ + plane * iz0, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, tw_r_, tile_r_};
+      prof_.begin(stream_);
+      launch_axis2<T>(plan_r_.n, r, g, stream_);
+      prof_.end(stream_, "kinetic_r", 2.0 * sizeof(V) * plane * g);
+      ++launches_;
+      kinetic_xy(half, with_gas, static_cast<long long>(iz0) * s_.nr, static_cast<long long>(g) * s_.nr);
+    }
   }
 
   // Specular grid: r forward, Z forward * factor * inverse, r inverse (* W factors).
@@ -793,8 +815,9 @@ class Step final : public StepBase {
     axis(name, bytes, psi_, outer, plan, tw, inner, factor, spo::kFactorAxis, spo::kFwdFactorInv, nullptr);
   }
 
-  // T_xy, optionally with the gas-phase potential step fused.
-  void kinetic_xy(bool half, bool with_gas) {
+  // T_xy, optionally with the gas-phase potential step fused; over the points izr in [izr_first,
+  // izr_first + n_izr) (n_izr < 0: all of them; a range needs the register kernel).
+  void kinetic_xy(bool half, bool with_gas, long long izr_first = 0, long long n_izr = -1) {
     spo::XyArgs<T> x{};
     x.psi = psi_;
     x.n_rot = s_.n_rot;
@@ -814,6 +837,14 @@ class Step final : public StepBase {
     x.opt_z = opt_z_;
     x.gas_step = gas_step_;
     x.tile = tile_xy_;
+    if (n_izr >= 0) {
+      x.izr_offset = izr_first;
+      prof_.begin(stream_);
+      require(launch_xy2<T>(x, n_izr, stream_), "kinetic_xy: a range of points needs the register kernel");
+      prof_.end(stream_, "kinetic_xy", 2.0 * sizeof(V) * n_izr * s_.n_xy() * s_.n_rot);
+      ++launches_;
+      return;
+    }
     const dim3 xg((s_.n_rot + xy_tb_ - 1) / xy_tb_, static_cast<unsigned>(s_.n_zr()));
     prof_.begin(stream_);
     if (!(use_v2_ && launch_xy2<T>(x, s_.n_zr(), stream_))) spo::xy_pass_kernel<T><<<xg, 256, xy_smem_, stream_>>>(x);
@@ -890,6 +921,7 @@ class Step final : public StepBase {
   void autotune() {
     tile_z_ = tile_r_ = tile_xy_ = 0;
     zr_window_ = 0;
+    rxy_planes_ = 0;
     tiles_source_ = "default";
     if (!use_v2_) return;
     if (const char* env = std::getenv("SPO_B200_TILES")) {
@@ -900,6 +932,11 @@ class Step final : public StepBase {
     }
     if (const char* env = std::getenv("SPO_B200_ZR_WINDOW")) {  // lanes per Z+r window (0: two full passes)
       zr_window_ = std::max(0ll, std::stoll(env) / 32 * 32);
+      tiles_source_ = "fixed";
+    }
+    if (const char* env = std::getenv("SPO_B200_RXY_PLANES")) {  // Z planes per r+xy slab (0: full passes)
+      rxy_planes_ = std::max(0, std::stoi(env));
+      if (!(axis2_supported(s_.nr) && s_.nx == s_.ny && xy2_supported(s_.nx))) rxy_planes_ = 0;
       tiles_source_ = "fixed";
     }
     if (tiles_source_ == "fixed") return;
@@ -947,6 +984,30 @@ class Step final : public StepBase {
         }
       }
       zr_window_ = best;
+    }
+    // T_r and T_xy through L2, slabs of 1, 2 or 4 Z planes, against the full passes.
+    rxy_planes_ = 0;
+    if (zr_window_ == 0 && axis2_supported(s_.nr) && s_.nx == s_.ny && xy2_supported(s_.nx)) {
+      auto run = [&] {
+        if (rxy_planes_ > 0) {
+          kinetic_rxy_slabs(false, false);
+        } else {
+          kinetic_zr(false);
+          kinetic_xy(false, false);
+        }
+      };
+      float best_ms = time_launches(run, reps);
+      int best = 0;
+      for (const int g : {1, 2, 4}) {
+        if (g >= s_.nz) continue;
+        rxy_planes_ = g;
+        const float ms = time_launches(run, reps);
+        if (ms < 0.98f * best_ms) {
+          best = g;
+          best_ms = ms;
+        }
+      }
+      rxy_planes_ = best;
     }
     prof_.enable(was_on);
     launches_ = 0;
@@ -1483,6 +1544,7 @@ class Step final : public StepBase {
   std::string pot_source_ = "default";
   int tile_z_ = 0, tile_r_ = 0, tile_xy_ = 0;  // batch lanes per block of the register kinetic kernels (0: default)
   long long zr_window_ = 0;                     // lanes per Z+r window (0: two full passes)
+  int rxy_planes_ = 0;                          // Z planes per r+xy slab (0: full passes)
   std::string tiles_source_ = "default";
   // Asymptotic analysis (FP64).
   std::vector<cplx> shift_host_;

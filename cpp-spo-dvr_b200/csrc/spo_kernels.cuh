@@ -260,6 +260,7 @@ struct XyArgs {
   const Vec<T>* gas_step;  // (ir, irot): opt_r rot gas rot
   int tile;                // launch choice of the register-DFT xy kernel: rotational states per block
                            // (8, 16 or 32; 0: the default) for grids of more than 8 points per axis
+  long long izr_offset;    // register-DFT xy kernel: block y serves point izr = izr_offset + y
 };
 
 template <typename T>

@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2_kernel(XyArgs<T> a
   V* f = S + NXY * TB;                     // NXY
   const int b = threadIdx.x % TB;
   const int s = threadIdx.x / TB;
-  const long long izr = blockIdx.y;
+  const long long izr = a.izr_offset + blockIdx.y;
   const int irot = blockIdx.x * TB + b;
   const bool lane_ok = irot < a.n_rot;
   const long long col0 = izr * NXY;

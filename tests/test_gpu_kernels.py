@@ -191,3 +191,27 @@ def test_potential5_agrees_with_potential4(j_max):
         res.append(be.wave_packet_on_host())
         be.close()
     assert rel_l2(res[1][0], res[0][0]) < 2e-5 and rel_l2(res[1][1], res[0][1]) < 2e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rxy_slabs_are_bitwise_equal(precision, monkeypatch):
+    """T_r and T_xy slab by slab of Z planes (through L2), with the gas-phase step fused in the xy pass:
+    the same lines with the same operations as the full passes, so bitwise the same wave packet; slabs
+    of 1 and 3 planes (3 does not divide nz = 32: a partial last slab)."""
+    from spo_b200 import workload
+    case = workload.config_case({"nz": 32, "nr": 24, "nx": 16, "ny": 16, "j_max": 3, "mj_max": 3,
+                                 "nz_specular": 64, "nz_potential": 20})
+    rng = np.random.default_rng(17)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    out = []
+    for planes in ("0", "1", "3"):
+        monkeypatch.setenv("SPO_B200_RXY_PLANES", planes)
+        be = make(case, "v4", precision)
+        assert f"rxy_planes={planes}" in be.describe(), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    for k in (1, 2):
+        assert np.array_equal(out[0][0], out[k][0]) and np.array_equal(out[0][1], out[k][1]), k
