@@ -154,3 +154,28 @@ def test_potential_kernels_match_oracle(ref_case, name, kernels, monkeypatch):
     assert rel_l2(psi, read_c128(os.path.join(d, "psi_final.c128"), shp)) < tol_steps
     assert rel_l2(chi, chis[1]) < tol_steps
     be.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_checkpoint_restart_is_bitwise(ref_case, precision):
+    """Checkpoint/restart through the backend interface (wave_packet_on_host, then read_wave_packet into a
+    fresh handle), as the reference's checkpoint files do (io/checkpoint.hpp; its restart test
+    test_restart.cpp:241 wants split runs bitwise equal to straight ones): two analysis steps straight
+    equal one step, a restart and one more step, bit for bit. The mixed form's complex64 state widens
+    to complex128 on the host and narrows back exactly."""
+    d = ref_case("tiny_oblique")
+    case, be, _, _ = backend_for(d, precision=precision)
+    be.propagate_analysis_step()
+    be.propagate_analysis_step()
+    straight = be.wave_packet_on_host()
+    be.close()
+    case, be, _, _ = backend_for(d, precision=precision)
+    be.propagate_analysis_step()
+    psi, chi = be.wave_packet_on_host()
+    be.close()
+    from spo_b200 import B200Backend
+    with B200Backend(case, precision=precision) as again:
+        again.read_wave_packet(psi, chi)
+        again.propagate_analysis_step()
+        split = again.wave_packet_on_host()
+    assert np.array_equal(straight[0], split[0]) and np.array_equal(straight[1], split[1])
