@@ -344,7 +344,7 @@ void launch_pot3(int nphi, const spo::Pot2Args<T>& a, dim3 grid, unsigned thread
 }
 
 // The potential4 instantiation for (nphi, ntheta), or null: ntheta 16, 8 and 4 with 8, 16 and 32 columns
-// per chunk, nphi 8, 16 and 32.
+// per chunk, nphi 8, 16 and 32 (and 12 with ntheta 4, a phi grid of the C6v symmetry).
 template <typename T>
 using Pot4Kernel = void (*)(spo::Pot4Args<T>);
 template <typename T>
@@ -354,6 +354,7 @@ Pot4Kernel<T> pot4_kernel_for(int nphi, int nt) {
   if (nt == 8 && nphi == 16) return spo::potential4_kernel<T, 16, 8, 16>;
   if (nt == 8 && nphi == 32) return spo::potential4_kernel<T, 32, 8, 16>;
   if (nt == 4 && nphi == 8) return spo::potential4_kernel<T, 8, 4, 32>;
+  if (nt == 4 && nphi == 12) return spo::potential4_kernel<T, 12, 4, 32>;  // C6v grids
   return nullptr;
 }
 
@@ -368,6 +369,7 @@ Pot5Kernel<T> pot5_kernel_for(int nphi, int nt) {
     if (nt == 16 && nphi == 32) return spo::potential5_kernel<T, 32, 16, 8>;
     if (nt == 8 && nphi == 16) return spo::potential5_kernel<T, 16, 8, 16>;
     if (nt == 4 && nphi == 8) return spo::potential5_kernel<T, 8, 4, 32>;
+    if (nt == 4 && nphi == 12) return spo::potential5_kernel<T, 12, 4, 32>;
     return nullptr;
   }
 }

@@ -20,7 +20,8 @@ for sub in ("", "cpp-spo-dvr_b200", "oracle"):
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 REF_TOOL = os.path.join(ROOT, "oracle", "_ref", "spo_ref_tool")
 REF_FFT_CHECK = os.path.join(ROOT, "oracle", "_ref", "ref_fft_check")
-TINY_CASES = ["tiny_hardwall", "tiny_dailight", "tiny_dailight_hetero", "tiny_oblique", "tiny_dailight_sym"]
+TINY_CASES = ["tiny_hardwall", "tiny_dailight", "tiny_dailight_hetero", "tiny_oblique", "tiny_dailight_sym",
+              "tiny_dailight_hetero_sym"]
 
 
 def pytest_configure(config):
