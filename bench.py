@@ -223,6 +223,70 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+# Shapes of the ensemble workload, from the configuration-4 ranges: Z 96-128, r 40-48, x = y 12-16,
+# theta 12-16 and phi 24-32 (heteronuclear JMax = MJMax 11-15), specular Z grid 512.
+ENSEMBLE_SHAPES = [
+    {"nz": 96, "nr": 40, "nx": 12, "ny": 12, "j_max": 11, "mj_max": 11, "nz_potential": 63},
+    {"nz": 112, "nr": 48, "nx": 12, "ny": 12, "j_max": 13, "mj_max": 13, "nz_potential": 74},
+    {"nz": 128, "nr": 40, "nx": 16, "ny": 16, "j_max": 11, "mj_max": 11, "nz_potential": 84},
+    {"nz": 128, "nr": 48, "nx": 16, "ny": 16, "j_max": 15, "mj_max": 15, "nz_potential": 84},
+]
+
+
+def run_ensemble(args):
+    """32 mixed-form wave packets of uneven grids (8 of each shape), one CUDA graph launch per analysis
+    step (spo_ensemble_*), against the same members stepped one after another."""
+    import numpy as np
+    import torch
+
+    from spo_b200 import B200Backend, Ensemble, workload
+
+    torch.cuda.set_device(0)
+    members, points = [], 0
+    for shape in ENSEMBLE_SHAPES:
+        case = workload.config_case(shape)
+        chi0 = np.ascontiguousarray(case.a["chi_initial"].reshape(case.chi_shape))
+        for _ in range(8):
+            be = B200Backend(case, precision="mixed")
+            be.read_wave_packet(None, chi0)
+            members.append(be)
+            points += case.n_points
+        case.a.clear()  # the descriptor's host tables are only read by spo_create
+    steps_per_analysis = members[0].case.steps_per_analysis
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    with Ensemble(members) as ens:
+        for _ in range(args.warmup):
+            ens.propagate_analysis_step()
+        # the ensemble step synchronises its own stream, so wall-clock events on the current stream bracket it
+        ms_graph = timed(ens.propagate_analysis_step, args.steps)
+        launches = ens.launch_count()
+    ms_seq = timed(lambda: [m.propagate_analysis_step() for m in members], args.steps)
+    for m in members:
+        m.close()
+    rate = points * steps_per_analysis * args.steps / (ms_graph / 1000.0)
+    print(json.dumps({
+        "metric": METRIC + " (ensemble)", "value": rate, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_graph / args.steps, "higher_is_better": True, "dtype": "c64",
+        "data": "synthetic", "config": {"workload": "32 mixed-form packets of the configuration-4 size ranges (8 each "
+                                                    "of 4 shapes), one graph launch per analysis step",
+                                        "shapes": ENSEMBLE_SHAPES, "points": points},
+        "one_after_another": {"value": points * steps_per_analysis * args.steps / (ms_seq / 1000.0),
+                              "ms_per_step": ms_seq / args.steps},
+        "gpu_launches": launches * args.steps,
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,12 +294,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config3", choices=["config3", "small"],
+    ap.add_argument("--workload", default="config3", choices=["config3", "small", "ensemble"],
                     help="small: the config-2 tables on nX = nY = 8 (psi 0.8 GB mixed, above L2), for profiler captures")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "ensemble":
+        if rank == 0:
+            run_ensemble(args)
         return
 
     import torch
