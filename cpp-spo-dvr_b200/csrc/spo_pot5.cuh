@@ -303,36 +303,49 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
       pending |= 2u;
     }
 
-    // ---- transposed theta contraction, rot(dt/2), store
-    for (int irot = tid; irot < n_rot; irot += NTH) {
-      const int slot = irot_slot[irot];
-      T acc[CB][2];
+    // ---- transposed theta contraction, rot(dt/2), store: two rotational states per pass (irot and
+    // irot + NTH), their sums interleaved as independent chains
+    for (int ia = tid; ia < n_rot; ia += 2 * NTH) {
+      const int ib = ia + NTH;
+      const bool has_b = ib < n_rot;
+      const int ibb = has_b ? ib : ia;
+      T acc[2][CB][2];
 #pragma unroll
-      for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = 0;
-      const T* lrow = L + irot * LDL;
-      const V* ys = X + slot * SS;
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int c = 0; c < CB; ++c) acc[u][c][0] = acc[u][c][1] = 0;
+      const T* lrow[2] = {L + ia * LDL, L + ibb * LDL};
+      const V* ys[2] = {X + irot_slot[ia] * SS, X + irot_slot[ibb] * SS};
 #pragma unroll 1
       for (int kq = 0; kq < QUADS; ++kq) {
-        T l[4];
-        ld4(lrow + 4 * kq, l);
+        T l[2][4];
+        ld4(lrow[0] + 4 * kq, l[0]);
+        ld4(lrow[1] + 4 * kq, l[1]);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const V* y = ys + (kq + QUADS * q) * CB;
 #pragma unroll
           for (int c = 0; c < CB; c += 2) {
-            V y0, y1;
-            ld2c(y + c, y0, y1);
-            acc[c][0] += l[q] * y0.x;
-            acc[c][1] += l[q] * y0.y;
-            acc[c + 1][0] += l[q] * y1.x;
-            acc[c + 1][1] += l[q] * y1.y;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              V y0, y1;
+              ld2c(ys[u] + (kq + QUADS * q) * CB + c, y0, y1);
+              acc[u][c][0] += l[u][q] * y0.x;
+              acc[u][c][1] += l[u][q] * y0.y;
+              acc[u][c + 1][0] += l[u][q] * y1.x;
+              acc[u][c + 1][1] += l[u][q] * y1.y;
+            }
           }
         }
       }
-      const V rh = a.rot_half[ir * n_rot + irot];
 #pragma unroll
-      for (int c = 0; c < CB; ++c)
-        if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, cmake<V>(acc[c][0], acc[c][1]));
+      for (int u = 0; u < 2; ++u) {
+        const int irot = u == 0 ? ia : ib;
+        if (u == 1 && !has_b) break;
+        const V rh = a.rot_half[ir * n_rot + irot];
+#pragma unroll
+        for (int c = 0; c < CB; ++c)
+          if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, cmake<V>(acc[u][c][0], acc[u][c][1]));
+      }
     }
   }
 }
