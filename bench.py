@@ -233,6 +233,13 @@ ENSEMBLE_SHAPES = [
 ]
 
 
+# DRAM bytes per algorithmic byte of the mixed-form potential kernel (potential5), from one ncu capture of
+# the small case (nX = nY = 8): dram__bytes_read.sum + dram__bytes_write.sum = 1.586 + 0.500 GB against
+# 2.114 GB algorithmic (interaction-region psi read and written once, the exp(i A) table read once). The
+# traffic grows with the columns processed, so the ratio carries over to configuration 3.
+POTENTIAL_DRAM_PER_ALGORITHMIC = (1.586e9 + 0.4998e9) / 2.114e9
+
+
 def run_ensemble(args):
     """32 mixed-form wave packets of uneven grids (8 of each shape), one CUDA graph launch per analysis
     step (spo_ensemble_*), against the same members stepped one after another."""
@@ -365,7 +372,12 @@ def main():
                                   "avg_ms": round(r["ms"] / r["launches"], 5)} for r in res["fp64"]["records"]]},
             "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
             "roofline": {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": top["bytes_per_launch"] * POTENTIAL_DRAM_PER_ALGORITHMIC
+                         if top["name"] == "potential" else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one potential5 launch "
+                                           "on the small case (nX = nY = 8: 2.086 GB for 2.114 GB algorithmic), "
+                                           "scaled to this launch by the columns processed",
                          "bytes_per_launch": top["bytes_per_launch"], "avg_launch_ms": avg_ms,
                          "share_of_kernel_time": top["ms"] / total_kernel_ms},
             "step_roofline": {"bytes_per_time_step": b_step, "achieved": step_gbs, "peak": peak, "unit": "GB/s",
