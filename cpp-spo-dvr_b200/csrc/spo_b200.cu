@@ -29,6 +29,7 @@
 #include "spo_regfft.cuh"
 #include "spo_pot4.cuh"
 #include "spo_pot5.cuh"
+#include "spo_persist.cuh"
 
 namespace {
 
@@ -157,6 +158,19 @@ std::size_t smem_optin_bytes() {
   return static_cast<std::size_t>(optin);
 }
 
+// Blocks of a persistent kernel: the SMs times the blocks that fit on one (looked up once per kernel).
+template <typename K>
+long long persistent_blocks(K kernel, int threads, std::size_t smem, int& cached) {
+  if (cached <= 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem), "occupancy");
+    cached = std::max(1, sms * per_sm);
+  }
+  return cached;
+}
+
 template <typename T, int N1, int N2, int TB>
 bool launch_axis2_tb(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
   constexpr int NS = N1 > N2 ? N1 : N2;
@@ -164,6 +178,16 @@ bool launch_axis2_tb(const spo::Axis2Args<T>& a, long long outer, cudaStream_t s
   const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(N) * TB + 2 * N);
   static unsigned long long configured = 0;
   allow_smem(spo::axis2_kernel<T, N1, N2, TB>, smem, configured, "axis2 smem");
+  if (a.persistent && a.window == 0) {
+    static unsigned long long configured_p = 0;
+    static int blocks_p = 0;
+    allow_smem(spo::axis2p_kernel<T, N1, N2, TB>, smem, configured_p, "axis2p smem");
+    const long long lane_blocks = (a.inner + TB - 1) / TB;
+    const long long n_tiles = outer * lane_blocks;
+    const long long grid = std::min(n_tiles, persistent_blocks(spo::axis2p_kernel<T, N1, N2, TB>, TB * NS, smem, blocks_p));
+    spo::axis2p_kernel<T, N1, N2, TB><<<static_cast<unsigned>(grid), TB * NS, smem, stream>>>(a, lane_blocks, n_tiles);
+    return true;
+  }
   if (a.window > 0) {  // lane windows: groups x ceil(window / TB) blocks
     spo::Axis2Args<T> w = a;
     w.blocks_per_group = static_cast<int>((a.window + TB - 1) / TB);
@@ -233,6 +257,16 @@ template <typename T, int NX, int NY, int TB>
 void launch_xy2_tb(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream) {
   constexpr int NS = NX > NY ? NX : NY;
   const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(NX * NY) * TB + NX * NY);
+  if (a.persistent) {
+    static unsigned long long configured_p = 0;
+    static int blocks_p = 0;
+    allow_smem(spo::xy2p_kernel<T, NX, NY, TB>, smem, configured_p, "xy2p smem");
+    const long long rot_tiles = (a.n_rot + TB - 1) / TB;
+    const long long n_tiles = n_zr * rot_tiles;
+    const long long grid = std::min(n_tiles, persistent_blocks(spo::xy2p_kernel<T, NX, NY, TB>, TB * NS, smem, blocks_p));
+    spo::xy2p_kernel<T, NX, NY, TB><<<static_cast<unsigned>(grid), TB * NS, smem, stream>>>(a, rot_tiles, n_tiles);
+    return;
+  }
   static unsigned long long configured = 0;
   allow_smem(spo::xy2_kernel<T, NX, NY, TB>, smem, configured, "xy2 smem");
   const dim3 grid(static_cast<unsigned>((a.n_rot + TB - 1) / TB), static_cast<unsigned>(n_zr));
@@ -543,7 +577,8 @@ class Step final : public StepBase {
       out += " potential=potential2<nphi=" + std::to_string(s_.nphi) + ",cb=" + std::to_string(pot2_cb_) + ">";
     else
       out += " potential=potential(general)";
-    out += " zr_window=" + std::to_string(zr_window_) + " rxy_planes=" + std::to_string(rxy_planes_) + " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
+    out += std::string(" persistent=") + (persist_z_ ? "z" : "") + (persist_r_ ? "r" : "") + (persist_xy_ ? "xy" : "") +
+           " zr_window=" + std::to_string(zr_window_) + " rxy_planes=" + std::to_string(rxy_planes_) + " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
     return out;
   }
 
@@ -737,11 +772,13 @@ class Step final : public StepBase {
   // is still in L2 when the xy pass reads it.
   void kinetic_rxy_slabs(bool half, bool with_gas) {
     const double b = 2.0 * sizeof(V) * s_.n_psi();
-    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, tile_z_);
+    axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, half ? zk_half_ : zk_full_, tile_z_,
+             persist_z_);
     const long long plane = static_cast<long long>(s_.nr) * s_.n_xy() * s_.n_rot;
     for (int iz0 = 0; iz0 < s_.nz; iz0 += rxy_planes_) {
       const int g = std::min(rxy_planes_, s_.nz - iz0);
       spo::Axis2Args<T> r{psi_ + plane * iz0, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, tw_r_, tile_r_};
+      r.persistent = persist_r_ ? 1 : 0;
       prof_.begin(stream_);
       launch_axis2<T>(plan_r_.n, r, g, stream_);
       prof_.end(stream_, "kinetic_r", 2.0 * sizeof(V) * plane * g);
@@ -769,8 +806,8 @@ class Step final : public StepBase {
     const V* zf = half ? zk_half_ : zk_full_;
     const V* rf = half ? rk_half_ : rk_full_;
     if (zr_window_ == 0) {
-      axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zf, tile_z_);
-      axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rf, tile_r_);
+      axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zf, tile_z_, persist_z_);
+      axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rf, tile_r_, persist_r_);
       return;
     }
     const long long lanes = s_.n_xy() * s_.n_rot;  // contiguous values per (Z, r) point
@@ -805,9 +842,10 @@ class Step final : public StepBase {
   // A kinetic axis pass over psi: the register-DFT kernel for its length when instantiated, else the
   // general Stockham kernel.
   void axis_psi(const char* name, double bytes, long long outer, const spo::FftPlan& plan, const V* tw,
-                long long inner, const V* factor, int tile) {
+                long long inner, const V* factor, int tile, bool persistent = false) {
     if (use_v2_ && axis2_supported(plan.n)) {
       spo::Axis2Args<T> a{psi_, inner, factor, tw, tile};
+      a.persistent = persistent ? 1 : 0;
       prof_.begin(stream_);
       launch_axis2<T>(plan.n, a, outer, stream_);
       prof_.end(stream_, name, bytes);
@@ -839,6 +877,7 @@ class Step final : public StepBase {
     x.opt_z = opt_z_;
     x.gas_step = gas_step_;
     x.tile = tile_xy_;
+    x.persistent = persist_xy_ ? 1 : 0;
     if (n_izr >= 0) {
       x.izr_offset = izr_first;
       prof_.begin(stream_);
@@ -924,6 +963,13 @@ class Step final : public StepBase {
     tile_z_ = tile_r_ = tile_xy_ = 0;
     zr_window_ = 0;
     rxy_planes_ = 0;
+    // The persistent forms are a fixed choice, not a timed one: they agree with the plain kernels to
+    // rounding only (the compiler may contract a complex product into FMAs differently in each), and a
+    // timed choice could make two runs of one case differ in the last bits. On configuration 3 the
+    // persistent xy pass (16 x 16) takes 1.50 ms against 1.66; the persistent Z and r passes are slower
+    // (2.17 against 1.43 ms for Z: 127 registers leave one block of 512 threads per SM).
+    persist_z_ = persist_r_ = false;
+    persist_xy_ = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx) && s_.nx >= 12;
     tiles_source_ = "default";
     if (!use_v2_) return;
     if (const char* env = std::getenv("SPO_B200_TILES")) {
@@ -934,6 +980,10 @@ class Step final : public StepBase {
     }
     if (const char* env = std::getenv("SPO_B200_ZR_WINDOW")) {  // lanes per Z+r window (0: two full passes)
       zr_window_ = std::max(0ll, std::stoll(env) / 32 * 32);
+      tiles_source_ = "fixed";
+    }
+    if (const char* env = std::getenv("SPO_B200_PERSISTENT")) {  // 1: the persistent kinetic kernels, 0: not
+      persist_z_ = persist_r_ = persist_xy_ = std::string(env) == "1";
       tiles_source_ = "fixed";
     }
     if (const char* env = std::getenv("SPO_B200_RXY_PLANES")) {  // Z planes per r+xy slab (0: full passes)
@@ -1547,6 +1597,7 @@ class Step final : public StepBase {
   int tile_z_ = 0, tile_r_ = 0, tile_xy_ = 0;  // batch lanes per block of the register kinetic kernels (0: default)
   long long zr_window_ = 0;                     // lanes per Z+r window (0: two full passes)
   int rxy_planes_ = 0;                          // Z planes per r+xy slab (0: full passes)
+  bool persist_z_ = false, persist_r_ = false, persist_xy_ = false;  // persistent forms of the passes
   std::string tiles_source_ = "default";
   // Asymptotic analysis (FP64).
   std::vector<cplx> shift_host_;

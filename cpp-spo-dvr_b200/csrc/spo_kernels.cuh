@@ -261,6 +261,7 @@ struct XyArgs {
   int tile;                // launch choice of the register-DFT xy kernel: rotational states per block
                            // (8, 16 or 32; 0: the default) for grids of more than 8 points per axis
   long long izr_offset;    // register-DFT xy kernel: block y serves point izr = izr_offset + y
+  int persistent;          // launch choice: the persistent form of the register-DFT xy kernel (xy2p_kernel)
 };
 
 template <typename T>

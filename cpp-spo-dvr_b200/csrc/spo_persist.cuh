@@ -1,0 +1,186 @@
+// Persistent forms of the register kinetic kernels: a grid of (SMs x resident blocks) loops over the
+// passes' tiles, and each thread requests the first-level values of its next tile into registers before
+// it transforms the current one, so the loads of tile k + 1 overlap the DFTs and the stores of tile k.
+// A tile's lines go through exactly the operations of axis2_kernel / xy2_kernel (spo_regfft.cuh), in
+// the same order: the two forms give the same wave packet bit for bit, and the autotuner may take
+// either.
+#pragma once
+
+#include "spo_regfft.cuh"
+
+namespace spo {
+
+// T_Z or T_r as axis2_kernel (whole passes, no lane windows): tiles (outer o, lanes i0 .. i0 + TB) in the
+// order o * lane_blocks + i0 / TB.
+template <typename T, int N1, int N2, int TB>
+__global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2p_kernel(Axis2Args<T> a, long long lane_blocks,
+                                                                       long long n_tiles) {
+  using V = Vec<T>;
+  constexpr int N = N1 * N2;
+  constexpr int NS = N1 > N2 ? N1 : N2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* Y = reinterpret_cast<V*>(smem_raw);
+  V* f = Y + N * TB;
+  V* tw = f + N;
+  const int b = threadIdx.x % TB;
+  const int s = threadIdx.x / TB;
+  const long long stride = a.inner;
+  auto locate = [&](long long tile, long long& base, bool& ok) {
+    const long long o = tile / lane_blocks;
+    const long long i0 = (tile - o * lane_blocks) * TB;
+    base = o * N * a.inner + i0 + b;
+    ok = i0 + b < a.inner;
+  };
+  auto fetch = [&](long long base, bool ok, V (&x)[N1]) {
+    if (s < N2) {
+      const int n2 = s;
+      static_for<0, N1>([&](auto n1) {
+        x[n1] = ok ? a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] : cmake<V>(0, 0);
+      });
+    }
+  };
+  for (int k = threadIdx.x; k < N; k += TB * NS) {
+    f[k] = a.factor[k];
+    tw[k] = a.tw[k];
+  }
+  __syncthreads();
+  long long tile = blockIdx.x, base = 0;
+  bool lane_ok = false;
+  V x[N1];
+  if (tile < n_tiles) {
+    locate(tile, base, lane_ok);
+    fetch(base, lane_ok, x);
+  }
+  for (; tile < n_tiles; tile += gridDim.x) {
+    const long long next = tile + gridDim.x;
+    long long nbase = 0;
+    bool nok = false;
+    V xn[N1];
+    if (next < n_tiles) {
+      locate(next, nbase, nok);
+      fetch(nbase, nok, xn);
+    }
+    // forward, level 1
+    if (s < N2) {
+      const int n2 = s;
+      rdft<N1, -1>(x);
+      static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : cmul(x[k1], tw[n2 * k1]); });
+    }
+    __syncthreads();
+    // forward level 2, factor, inverse level 2
+    if (s < N1) {
+      const int k1 = s;
+      V y[N2];
+      static_for<0, N2>([&](auto n2) { y[n2] = Y[(n2 * N1 + k1) * TB + b]; });
+      rdft<N2, -1>(y);
+      static_for<0, N2>([&](auto k2) { y[k2] = cmul(f[k1 + N1 * k2], y[k2]); });
+      rdft<N2, +1>(y);
+      static_for<0, N2>([&](auto n2) { Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : cmul(y[n2], cconj(tw[n2 * k1])); });
+    }
+    __syncthreads();
+    // inverse level 1, store
+    if (s < N2 && lane_ok) {
+      const int n2 = s;
+      V z[N1];
+      static_for<0, N1>([&](auto k1) { z[k1] = Y[(n2 * N1 + k1) * TB + b]; });
+      rdft<N1, +1>(z);
+      static_for<0, N1>([&](auto n1) { a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] = z[n1]; });
+    }
+    __syncthreads();  // Y is read before the next tile's first level writes it
+    static_for<0, N1>([&](auto n1) { x[n1] = xn[n1]; });
+    base = nbase;
+    lane_ok = nok;
+  }
+}
+
+// T_xy as xy2_kernel over the points izr_offset .. izr_offset + n_zr: tiles (point, rotational states
+// r0 .. r0 + TB) in the order p * rot_tiles + r0 / TB.
+template <typename T, int NX, int NY, int TB>
+__global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2p_kernel(XyArgs<T> a, long long rot_tiles,
+                                                                     long long n_tiles) {
+  using V = Vec<T>;
+  constexpr int NXY = NX * NY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* S = reinterpret_cast<V*>(smem_raw);  // NXY * TB
+  V* f = S + NXY * TB;                     // NXY
+  const int b = threadIdx.x % TB;
+  const int s = threadIdx.x / TB;
+  auto locate = [&](long long tile, long long& izr, int& irot, bool& ok) {
+    const long long p = tile / rot_tiles;
+    izr = a.izr_offset + p;
+    irot = static_cast<int>(tile - p * rot_tiles) * TB + b;
+    ok = irot < a.n_rot;
+  };
+  auto fetch = [&](long long izr, int irot, bool ok, V (&x)[NY]) {
+    if (s < NX) {
+      const int ix = s;
+      const long long col0 = izr * NXY;
+      static_for<0, NY>([&](auto iy) { x[iy] = ok ? a.psi[(col0 + ix * NY + iy) * a.n_rot + irot] : cmake<V>(0, 0); });
+    }
+  };
+  for (int k = threadIdx.x; k < NXY; k += blockDim.x) f[k] = a.factor[k];
+  __syncthreads();
+  long long tile = blockIdx.x, izr = 0;
+  int irot = 0;
+  bool lane_ok = false;
+  V x[NY];
+  if (tile < n_tiles) {
+    locate(tile, izr, irot, lane_ok);
+    fetch(izr, irot, lane_ok, x);
+  }
+  for (; tile < n_tiles; tile += gridDim.x) {
+    const long long next = tile + gridDim.x;
+    long long nizr = 0;
+    int nirot = 0;
+    bool nok = false;
+    V xn[NY];
+    if (next < n_tiles) {
+      locate(next, nizr, nirot, nok);
+      fetch(nizr, nirot, nok, xn);
+    }
+    const long long col0 = izr * NXY;
+    if (s < NX) {
+      const int ix = s;
+      if (a.shift_f)
+        static_for<0, NY>([&](auto iy) {
+          if (lane_ok) x[iy] = cmul(x[iy], a.shift_f[ix * NY + iy]);
+        });
+      rdft<NY, -1>(x);
+      static_for<0, NY>([&](auto ky) { S[(ix * NY + ky) * TB + b] = x[ky]; });
+    }
+    __syncthreads();
+    if (s < NY) {
+      const int ky = s;
+      V y[NX];
+      static_for<0, NX>([&](auto ix) { y[ix] = S[(ix * NY + ky) * TB + b]; });
+      rdft<NX, -1>(y);
+      static_for<0, NX>([&](auto kx) { y[kx] = cmul(f[kx * NY + ky], y[kx]); });
+      rdft<NX, +1>(y);
+      static_for<0, NX>([&](auto ix) { S[(ix * NY + ky) * TB + b] = y[ix]; });
+    }
+    __syncthreads();
+    if (s < NX && lane_ok) {
+      const int ix = s;
+      V z[NY];
+      static_for<0, NY>([&](auto ky) { z[ky] = S[(ix * NY + ky) * TB + b]; });
+      rdft<NY, +1>(z);
+      const bool gas = a.apply_gas && izr >= a.izr_gas_first;
+      const int ir = static_cast<int>(izr % a.nr);
+      V g = cmake<V>(1, 0);
+      if (gas) g = cscale(a.gas_step[ir * a.n_rot + irot], a.opt_z[izr / a.nr]);
+      static_for<0, NY>([&](auto iy) {
+        V v = z[iy];
+        if (a.shift_b) v = cmul(v, a.shift_b[ix * NY + iy]);
+        if (gas) v = cmul(g, v);
+        a.psi[(col0 + ix * NY + iy) * a.n_rot + irot] = v;
+      });
+    }
+    __syncthreads();  // S is read before the next tile's first level writes it
+    static_for<0, NY>([&](auto iy) { x[iy] = xn[iy]; });
+    izr = nizr;
+    irot = nirot;
+    lane_ok = nok;
+  }
+}
+
+}  // namespace spo

@@ -215,3 +215,32 @@ def test_rxy_slabs_are_bitwise_equal(precision, monkeypatch):
         be.close()
     for k in (1, 2):
         assert np.array_equal(out[0][0], out[k][0]) and np.array_equal(out[0][1], out[k][1]), k
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_kinetic_kernels_agree(precision, monkeypatch):
+    """The persistent forms of the register kinetic kernels (next tile's loads in flight during the
+    current tile) apply the same operations to every line, with the momentum shift of oblique incidence
+    and the fused gas-phase step included: the same wave packet to rounding (1e-13 FP64, 2e-6 mixed; not
+    bitwise, the compiler's FMA contractions may differ between the two kernels)."""
+    from spo_b200 import workload
+    case = workload.config_case({"nz": 128, "nr": 24, "nx": 16, "ny": 16, "j_max": 3, "mj_max": 3,
+                                 "nz_specular": 256, "nz_potential": 40})
+    rng = np.random.default_rng(23)
+    n_xy = case.nx * case.ny
+    phase = np.exp(1j * rng.uniform(0, 2 * np.pi, n_xy))
+    case.a["shift_forward"] = phase
+    case.a["shift_backward"] = np.conj(phase)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    out = []
+    for persistent in ("0", "1"):
+        monkeypatch.setenv("SPO_B200_PERSISTENT", persistent)
+        be = make(case, "v4", precision)
+        assert ("persistent=zrxy" in be.describe()) == (persistent == "1"), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    tol = 1e-13 if precision == "fp64" else 2e-6
+    assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol
