@@ -165,12 +165,21 @@ def measure(case, precision, steps, warmup, device, world):
 
 
 def reduce_max(x, world, device):
+    """The maximum of x over the ranks (every rank takes part; NCCL on the GPUs, any other backend on
+    the host)."""
     if world == 1:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    on_gpu = torch.distributed.get_backend() == "nccl"
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}" if on_gpu else "cpu")
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(points, time_steps, ms_max, world):
+    """Whole-job grid-point-steps/s of `world` replicas, each advancing `points` grid points by
+    `time_steps`, timed by the slowest rank (ms_max)."""
+    return world * points * time_steps / (ms_max / 1000.0)
 
 
 def cpu_sample_input(nx: int):
@@ -332,8 +341,8 @@ def main():
     for precision, r in res.items():
         ms = reduce_max(r["ms"], world, local)
         e2e_ms = reduce_max(r["e2e_ms"], world, local)
-        out[precision] = {"ms": ms, "value": world * points * time_steps / (ms / 1000.0),
-                          "e2e": world * points * time_steps / (e2e_ms / 1000.0)}
+        out[precision] = {"ms": ms, "value": job_rate(points, time_steps, ms, world),
+                          "e2e": job_rate(points, time_steps, e2e_ms, world)}
     if world > 1:
         torch.distributed.barrier()
     if rank == 0:
