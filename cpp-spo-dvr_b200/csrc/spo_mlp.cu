@@ -8,7 +8,8 @@
 //     canonical K-major layout without swizzle (8-row x 16-byte core matrices: K chunks LBO bytes
 //     apart, 8-row groups SBO = 128 bytes apart), make the writes visible to the tensor core
 //     (fence.proxy.async), and one thread issues four tcgen05.mma (M 128, N, K 16) and a
-//     tcgen05.commit on an mbarrier; every thread waits for it (bounded) before the next chunk;
+//     tcgen05.commit on the stage's mbarrier; two stages alternate, so chunk k + 1 is staged while
+//     the tensor core multiplies chunk k (a stage is rewritten after its previous commit, bounded wait);
 //   - epilogue: each warp reads its 32 accumulator lanes (tcgen05.ld 32x32b, 16 columns at a time)
 //     and writes FP32, BF16, or bias + SiLU (pre-activation FP32, activation BF16);
 //   - split K: blockIdx.y takes a share of the K chunks and writes its own FP32 partial, summed in a
@@ -138,23 +139,26 @@ struct GemmArgs {
 };
 
 constexpr int kBM = 128, kBK = 64, kBNMax = 256;
-constexpr std::size_t kGemmSmem = static_cast<std::size_t>(kBM + kBNMax) * kBK * 2 + 64;
-// Launched with more shared memory than it uses: at most two blocks per SM, the number whose 256
-// tensor-memory columns fit the SM's 512 together.
-constexpr std::size_t kGemmLaunchSmem = 80 * 1024;
-static_assert(kGemmSmem <= kGemmLaunchSmem, "the launch covers the kernel's shared memory");
+constexpr std::size_t kStageBytes = static_cast<std::size_t>(kBM + kBNMax) * kBK * 2;  // one A and one B chunk
+constexpr std::size_t kGemmSmem = 2 * kStageBytes + 64;                                  // two stages, barriers
+// At most two blocks per SM: the number whose 256 tensor-memory columns fit the SM's 512 together.
+constexpr std::size_t kGemmLaunchSmem = kGemmSmem;
+static_assert(3 * kGemmLaunchSmem > 228 * 1024, "two blocks per SM at most");
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 
+// Two stages: while the tensor core multiplies chunk k (stage k % 2), the threads stage chunk k + 1 in
+// the other buffer, after the commit of chunk k - 1 (its previous user) has arrived.
 __global__ void __launch_bounds__(128) gemm_tn_kernel(GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* As = smem;                                // core (r8, kc) at (kc * 16 + r8) * 128
-  unsigned char* Bs = smem + kBM * kBK * 2;                // core (r8, kc) at (kc * 32 + r8) * 128
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (kBM + kBNMax) * kBK * 2);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kStageBytes);  // one per stage
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) tc::tmem_alloc(tslot, 256);
-  if (tid == 0) tc::mbar_init(bar, 1);
+  if (tid == 0) {
+    tc::mbar_init(bar, 1);
+    tc::mbar_init(bar + 1, 1);
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -165,41 +169,78 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(GemmArgs g) {
   const int nk = g.k / kBK;
   const int kc_first = static_cast<int>(static_cast<long long>(nk) * blockIdx.y / gridDim.y);
   const int kc_last = static_cast<int>(static_cast<long long>(nk) * (blockIdx.y + 1) / gridDim.y);
-  uint32_t phase = 0;
-  bool failed = false;
-  for (int kc = kc_first; kc < kc_last; ++kc) {
+  // A: core (r8, kc) at (kc * 16 + r8) * 128; B: core (r8, kc) at (kc * 32 + r8) * 128
+  // All of a thread's 16-byte loads of a chunk are issued before the first is stored.
+  auto stage = [&](int st, int kc) {
+    unsigned char* As = smem + st * kStageBytes;
+    unsigned char* Bs = As + kBM * kBK * 2;
     const int k0 = kc * kBK;
-    for (int p = tid; p < kBM * 8; p += 128) {
-      const int r = p >> 3, c = p & 7;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (m0 + r < g.m) v = *reinterpret_cast<const uint4*>(g.a + static_cast<long long>(m0 + r) * g.lda + k0 + 8 * c);
-      *reinterpret_cast<uint4*>(As + (c * (kBM / 8) + (r >> 3)) * 128 + (r & 7) * 16) = v;
+    constexpr int NA = kBM * 8 / 128, NB = kBNMax * 8 / 128;
+    uint4 va[NA], vb[NB];
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+      const int p = tid + 128 * i, r = p >> 3, c = p & 7;
+      va[i] = m0 + r < g.m ? *reinterpret_cast<const uint4*>(g.a + static_cast<long long>(m0 + r) * g.lda + k0 + 8 * c)
+                           : make_uint4(0, 0, 0, 0);
     }
-    for (int p = tid; p < g.n * 8; p += 128) {
-      const int r = p >> 3, c = p & 7;
-      const uint4 v = *reinterpret_cast<const uint4*>(g.b + static_cast<long long>(r) * g.ldb + k0 + 8 * c);
-      *reinterpret_cast<uint4*>(Bs + (c * (kBNMax / 8) + (r >> 3)) * 128 + (r & 7) * 16) = v;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+      const int p = tid + 128 * i, r = p >> 3, c = p & 7;
+      if (p < g.n * 8) vb[i] = *reinterpret_cast<const uint4*>(g.b + static_cast<long long>(r) * g.ldb + k0 + 8 * c);
     }
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+      const int p = tid + 128 * i, r = p >> 3, c = p & 7;
+      *reinterpret_cast<uint4*>(As + (c * (kBM / 8) + (r >> 3)) * 128 + (r & 7) * 16) = va[i];
+    }
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+      const int p = tid + 128 * i, r = p >> 3, c = p & 7;
+      if (p < g.n * 8) *reinterpret_cast<uint4*>(Bs + (c * (kBNMax / 8) + (r >> 3)) * 128 + (r & 7) * 16) = vb[i];
+    }
+    tc::fence_proxy_async();  // the generic writes, visible to the tensor core
+  };
+  uint32_t parity = 0;  // bit s: the phase parity of stage s's barrier
+  bool failed = false;
+  if (kc_first < kc_last) stage(0, kc_first);
+  tc::fence_before_sync();
+  __syncthreads();
+  for (int kc = kc_first; kc < kc_last; ++kc) {
+    const int st = (kc - kc_first) & 1;
     if (tid == 0) {
       tc::fence_after_sync();
-      const uint32_t a0 = tc::smem_addr(As), b0 = tc::smem_addr(Bs);
+      const uint32_t a0 = tc::smem_addr(smem + st * kStageBytes);
+      const uint32_t b0 = a0 + kBM * kBK * 2;
 #pragma unroll
       for (int s = 0; s < kBK / 16; ++s) {
         const uint64_t ad = tc::smem_desc(a0 + 2 * s * (kBM / 8) * 128, (kBM / 8) * 128, 128);
         const uint64_t bd = tc::smem_desc(b0 + 2 * s * (kBNMax / 8) * 128, (kBNMax / 8) * 128, 128);
         tc::mma_bf16(tmem, ad, bd, idesc, (kc > kc_first || s > 0) ? 1u : 0u);
       }
-      tc::commit(bar);
+      tc::commit(bar + st);
     }
-    const bool ok = tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(!ok)) {
-      failed = true;
-      break;
+    if (kc + 1 < kc_last) {
+      // the other stage's previous chunk (kc - 1) must be multiplied before it is overwritten
+      bool ok = true;
+      if (kc > kc_first) {
+        ok = tc::mbar_wait(bar + (st ^ 1), parity >> (st ^ 1) & 1u);
+        parity ^= 1u << (st ^ 1);
+      }
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      stage(st ^ 1, kc + 1);
     }
+    tc::fence_before_sync();
+    __syncthreads();
+  }
+  // The last chunk's commit: it arrives when every earlier tcgen05.mma of the issuing thread has
+  // completed, so the accumulator is final (the second-to-last commit needs no wait of its own).
+  if (!failed && kc_last > kc_first) {
+    const int last = (kc_last - kc_first - 1) & 1;
+    const bool ok = tc::mbar_wait(bar + last, parity >> last & 1u);
+    failed = __syncthreads_or(!ok) != 0;
   }
   tc::fence_after_sync();
   if (failed) {
