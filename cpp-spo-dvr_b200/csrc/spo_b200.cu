@@ -188,6 +188,15 @@ bool launch_axis2_tb(const spo::Axis2Args<T>& a, long long outer, cudaStream_t s
     spo::axis2p_kernel<T, N1, N2, TB><<<static_cast<unsigned>(grid), TB * NS, smem, stream>>>(a, lane_blocks, n_tiles);
     return true;
   }
+  if constexpr (N2 == 2 * N1) {
+    if (a.balanced && a.window == 0) {
+      static unsigned long long configured_b = 0;
+      allow_smem(spo::axis2b_kernel<T, N1, N2, TB>, smem, configured_b, "axis2b smem");
+      const dim3 grid(static_cast<unsigned>((a.inner + TB - 1) / TB), static_cast<unsigned>(outer));
+      spo::axis2b_kernel<T, N1, N2, TB><<<grid, TB * N1, smem, stream>>>(a);
+      return true;
+    }
+  }
   if (a.window > 0) {  // lane windows: groups x ceil(window / TB) blocks
     spo::Axis2Args<T> w = a;
     w.blocks_per_group = static_cast<int>((a.window + TB - 1) / TB);
@@ -243,6 +252,8 @@ bool axis2_has_tiles(int n) {
     default: return false;
   }
 }
+// Lengths N1 x 2 N1, which have the balanced form (axis2b_kernel).
+bool axis2_balanced(int n) { return n == 32 || n == 128; }
 bool axis2_supported(int n) {
   switch (n) {
     case 24: case 32: case 40: case 48: case 56: case 64: case 80: case 96: case 112: case 128: case 160: case 176:
@@ -554,15 +565,16 @@ class Step final : public StepBase {
 
   std::string describe() const override {
     auto lanes = [](int tile, bool has_tiles) { return "tb" + std::to_string(!has_tiles ? 32 : tile ? tile : 16); };
-    auto axis_name = [&](int n, int tile) {
+    auto axis_name = [&](int n, int tile, bool persistent) {
       if (!(use_v2_ && axis2_supported(n))) return std::string("axis_pass(general)");
-      return "axis2<" + std::to_string(n) + "," + lanes(tile, axis2_has_tiles(n)) + ">";
+      const char* form = zr_window_ > 0 ? "axis2" : persistent ? "axis2p" : balanced_ && axis2_balanced(n) ? "axis2b" : "axis2";
+      return form + std::string("<") + std::to_string(n) + "," + lanes(tile, axis2_has_tiles(n)) + ">";
     };
     std::string out = std::string(sizeof(T) == 8 ? "fp64" : "mixed");
-    out += " z=" + axis_name(s_.nz, tile_z_);
-    out += " r=" + axis_name(s_.nr, tile_r_);
+    out += " z=" + axis_name(s_.nz, tile_z_, persist_z_);
+    out += " r=" + axis_name(s_.nr, tile_r_, persist_r_);
     const bool xy2 = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx);
-    out += std::string(" xy=") + (xy2 ? "xy2<" + std::to_string(s_.nx) + "," + lanes(tile_xy_, s_.nx > 8) + ">"
+    out += std::string(" xy=") + (xy2 ? std::string(persist_xy_ ? "xy2p<" : "xy2<") + std::to_string(s_.nx) + "," + lanes(tile_xy_, s_.nx > 8) + ">"
                                       : std::string("xy_pass(general)"));
     if (pot_kind_ == 5)
       out += " potential=potential5<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
@@ -577,7 +589,7 @@ class Step final : public StepBase {
       out += " potential=potential2<nphi=" + std::to_string(s_.nphi) + ",cb=" + std::to_string(pot2_cb_) + ">";
     else
       out += " potential=potential(general)";
-    out += std::string(" persistent=") + (persist_z_ ? "z" : "") + (persist_r_ ? "r" : "") + (persist_xy_ ? "xy" : "") +
+    out += std::string(" balanced=") + (balanced_ ? "1" : "0") + " persistent=" + (persist_z_ ? "z" : "") + (persist_r_ ? "r" : "") + (persist_xy_ ? "xy" : "") +
            " zr_window=" + std::to_string(zr_window_) + " rxy_planes=" + std::to_string(rxy_planes_) + " tiles=" + tiles_source_ + " potential_choice=" + pot_source_;
     return out;
   }
@@ -806,8 +818,8 @@ class Step final : public StepBase {
     const V* zf = half ? zk_half_ : zk_full_;
     const V* rf = half ? rk_half_ : rk_full_;
     if (zr_window_ == 0) {
-      axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zf, tile_z_, persist_z_);
-      axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rf, tile_r_, persist_r_);
+      axis_psi("kinetic_z", b, 1, plan_z_, tw_z_, s_.n_xy() * s_.nr * s_.n_rot, zf, tile_z_, persist_z_, balanced_);
+      axis_psi("kinetic_r", b, s_.nz, plan_r_, tw_r_, s_.n_xy() * s_.n_rot, rf, tile_r_, persist_r_, balanced_);
       return;
     }
     const long long lanes = s_.n_xy() * s_.n_rot;  // contiguous values per (Z, r) point
@@ -842,10 +854,11 @@ class Step final : public StepBase {
   // A kinetic axis pass over psi: the register-DFT kernel for its length when instantiated, else the
   // general Stockham kernel.
   void axis_psi(const char* name, double bytes, long long outer, const spo::FftPlan& plan, const V* tw,
-                long long inner, const V* factor, int tile, bool persistent = false) {
+                long long inner, const V* factor, int tile, bool persistent = false, bool balanced = false) {
     if (use_v2_ && axis2_supported(plan.n)) {
       spo::Axis2Args<T> a{psi_, inner, factor, tw, tile};
       a.persistent = persistent ? 1 : 0;
+      a.balanced = balanced ? 1 : 0;
       prof_.begin(stream_);
       launch_axis2<T>(plan.n, a, outer, stream_);
       prof_.end(stream_, name, bytes);
@@ -970,6 +983,10 @@ class Step final : public StepBase {
     // (2.17 against 1.43 ms for Z: 127 registers leave one block of 512 threads per SM).
     persist_z_ = persist_r_ = false;
     persist_xy_ = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx) && s_.nx >= 12;
+    // The balanced axis kernel (lengths N1 x 2 N1: 32 and 128) is a fixed choice for the same reason:
+    // Z = 128 on configuration 3 takes 1.38 ms against 1.43 (mixed), 2.69 against 2.71 (FP64). An explicit
+    // persistent request takes precedence over it.
+    balanced_ = use_v2_;
     tiles_source_ = "default";
     if (!use_v2_) return;
     if (const char* env = std::getenv("SPO_B200_TILES")) {
@@ -980,6 +997,10 @@ class Step final : public StepBase {
     }
     if (const char* env = std::getenv("SPO_B200_ZR_WINDOW")) {  // lanes per Z+r window (0: two full passes)
       zr_window_ = std::max(0ll, std::stoll(env) / 32 * 32);
+      tiles_source_ = "fixed";
+    }
+    if (const char* env = std::getenv("SPO_B200_BALANCED")) {  // 1: the balanced axis kernels (N2 = 2 N1), 0: not
+      balanced_ = std::string(env) == "1";
       tiles_source_ = "fixed";
     }
     if (const char* env = std::getenv("SPO_B200_PERSISTENT")) {  // 1: the persistent kinetic kernels, 0: not
@@ -1598,6 +1619,7 @@ class Step final : public StepBase {
   long long zr_window_ = 0;                     // lanes per Z+r window (0: two full passes)
   int rxy_planes_ = 0;                          // Z planes per r+xy slab (0: full passes)
   bool persist_z_ = false, persist_r_ = false, persist_xy_ = false;  // persistent forms of the passes
+  bool balanced_ = false;  // balanced axis kernels where N2 = 2 N1
   std::string tiles_source_ = "default";
   // Asymptotic analysis (FP64).
   std::vector<cplx> shift_host_;

@@ -1,9 +1,9 @@
 // Persistent forms of the register kinetic kernels: a grid of (SMs x resident blocks) loops over the
 // passes' tiles, and each thread requests the first-level values of its next tile into registers before
 // it transforms the current one, so the loads of tile k + 1 overlap the DFTs and the stores of tile k.
-// A tile's lines go through exactly the operations of axis2_kernel / xy2_kernel (spo_regfft.cuh), in
-// the same order: the two forms give the same wave packet bit for bit, and the autotuner may take
-// either.
+// A tile's lines go through the operations of axis2_kernel / xy2_kernel (spo_regfft.cuh) in the same
+// order; the forms agree to rounding (the compiler may contract the products of a complex multiply into
+// FMAs differently in each kernel), so which one a pass uses is a fixed choice, not a timed one.
 #pragma once
 
 #include "spo_regfft.cuh"
@@ -180,6 +180,70 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2p_kernel(XyArgs<T> 
     izr = nizr;
     irot = nirot;
     lane_ok = nok;
+  }
+}
+
+}  // namespace spo
+
+namespace spo {
+
+// T_Z or T_r as axis2_kernel for N2 = 2 N1 (whole passes, no lane windows), with every thread busy in
+// both levels: TB x N1 threads; thread (b, s) takes the first-level lines n2 = s and s + N1 of lane b
+// (two DFT_N1) and the second-level line k1 = s (one DFT_N2). In axis2_kernel (TB x N2 threads) half of
+// the threads wait at the barrier during the second level. Dynamic shared memory as axis2_kernel.
+template <typename T, int N1, int N2, int TB>
+__global__ void __launch_bounds__(TB * N1) axis2b_kernel(Axis2Args<T> a) {
+  using V = Vec<T>;
+  static_assert(N2 == 2 * N1, "the balanced form needs N2 = 2 N1");
+  constexpr int N = N1 * N2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* Y = reinterpret_cast<V*>(smem_raw);
+  V* f = Y + N * TB;
+  V* tw = f + N;
+  const int b = threadIdx.x % TB;
+  const int s = threadIdx.x / TB;
+  const long long i0 = static_cast<long long>(blockIdx.x) * TB;
+  const long long base = static_cast<long long>(blockIdx.y) * N * a.inner + i0 + b;
+  const long long stride = a.inner;
+  const bool lane_ok = i0 + b < a.inner;
+  for (int k = threadIdx.x; k < N; k += TB * N1) {
+    f[k] = a.factor[k];
+    tw[k] = a.tw[k];
+  }
+  __syncthreads();
+  // forward, level 1: lines n2 = s, s + N1
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int n2 = s + h * N1;
+    V x[N1];
+    static_for<0, N1>([&](auto n1) {
+      x[n1] = lane_ok ? a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] : cmake<V>(0, 0);
+    });
+    rdft<N1, -1>(x);
+    static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : cmul(x[k1], tw[n2 * k1]); });
+  }
+  __syncthreads();
+  // forward level 2, factor, inverse level 2: line k1 = s
+  {
+    const int k1 = s;
+    V y[N2];
+    static_for<0, N2>([&](auto n2) { y[n2] = Y[(n2 * N1 + k1) * TB + b]; });
+    rdft<N2, -1>(y);
+    static_for<0, N2>([&](auto k2) { y[k2] = cmul(f[k1 + N1 * k2], y[k2]); });
+    rdft<N2, +1>(y);
+    static_for<0, N2>([&](auto n2) { Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : cmul(y[n2], cconj(tw[n2 * k1])); });
+  }
+  __syncthreads();
+  // inverse level 1, store: lines n2 = s, s + N1
+  if (lane_ok) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int n2 = s + h * N1;
+      V x[N1];
+      static_for<0, N1>([&](auto k1) { x[k1] = Y[(n2 * N1 + k1) * TB + b]; });
+      rdft<N1, +1>(x);
+      static_for<0, N1>([&](auto n1) { a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] = x[n1]; });
+    }
   }
 }
 

@@ -209,6 +209,7 @@ struct Axis2Args {
   long long group_stride, lane_offset, window, line_stride, outer_stride;
   long long groups;  // host side: lane groups per line set (the launch has groups * blocks_per_group blocks)
   int persistent;    // launch choice: the persistent form (axis2p_kernel) for whole passes
+  int balanced;      // launch choice: the balanced form (axis2b_kernel, N2 = 2 N1) for whole passes
 };
 
 // Dynamic shared memory: (N TB + 2 N) values (axis2_smem).

@@ -101,7 +101,7 @@ def test_tile_widths_are_bitwise_equal(precision):
     out = []
     for tiles in ("8", "16", "32"):
         be = make(case, "v3", precision, tiles)
-        assert f"z=axis2<128,tb{tiles}>" in be.describe() and f"xy=xy2<16,tb{tiles}>" in be.describe(), be.describe()
+        assert f"z=axis2b<128,tb{tiles}>" in be.describe() and f"xy=xy2p<16,tb{tiles}>" in be.describe(), be.describe()
         be.read_wave_packet(psi0, chi0)
         be.propagate_analysis_step()
         out.append(be.wave_packet_on_host())
@@ -238,6 +238,35 @@ def test_persistent_kinetic_kernels_agree(precision, monkeypatch):
         monkeypatch.setenv("SPO_B200_PERSISTENT", persistent)
         be = make(case, "v4", precision)
         assert ("persistent=zrxy" in be.describe()) == (persistent == "1"), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    tol = 1e-13 if precision == "fp64" else 2e-6
+    assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nz,nr", [(128, 24), (48, 32)])
+def test_balanced_axis_kernel_agrees(nz, nr, precision, monkeypatch):
+    """The balanced axis kernel (lengths N1 x 2 N1: Z = 128 = 8 x 16, r = 32 = 4 x 8), in which every
+    thread takes two first-level lines and one second-level line, against the plain one (N2 threads per
+    lane, half of them idle in the second level): the same wave packet to rounding (1e-13 FP64, 2e-6
+    mixed)."""
+    from spo_b200 import workload
+    case = workload.config_case({"nz": nz, "nr": nr, "nx": 8, "ny": 8, "j_max": 3, "mj_max": 3,
+                                 "nz_specular": 2 * nz, "nz_potential": 40})
+    rng = np.random.default_rng(31)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    n = nz if nz == 128 else nr
+    axis = "z" if nz == 128 else "r"
+    out = []
+    for balanced in ("0", "1"):
+        monkeypatch.setenv("SPO_B200_BALANCED", balanced)
+        be = make(case, "v4", precision)
+        form = "axis2b" if balanced == "1" else "axis2"
+        assert f"{axis}={form}<{n}," in be.describe(), be.describe()
         be.read_wave_packet(psi0, chi0)
         be.propagate_analysis_step()
         out.append(be.wave_packet_on_host())
