@@ -11,6 +11,9 @@
 //   - exp(i A): each thread's phi line (NPHI contiguous values of its column's representative) into its
 //     own row of E (rows of NPHI + 2 values: 16-byte loads of 8 consecutive rows on distinct banks);
 //     issued for item k + 1 when item k's phi phase is done.
+//   - the item's rows of the scaling tables (opt_r rot(dt/2) and rot(dt/2) at its r point) with the
+//     columns; its opt_z value, incoming specular amplitude and sp2sc coefficients into registers when
+//     the copies are issued, so that no global load sits on the path between two barriers.
 // Per item: wait for F; scale it in place (absorbers, rot(dt/2), the specular wave into the initial
 // channel); forward theta sums (potential4's tiles, F read column-major); wait for E; phi DFT, exp(i A),
 // inverse DFT; transposed theta sums, rot(dt/2), store. The matrix rows are staged in shared memory as
@@ -91,15 +94,17 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
 }  // namespace pot5
 
 // Shared memory of potential5_kernel: 2 barriers (padded to 32 bytes), F (CB columns of n_rot + 2
-// values), E (NT CB rows of NPHI + 2 values), X (NPHI padded slot blocks), the matrix rows (n_rot rows
-// of NT + 4), irot -> slot (n_rot ints), the schedule (8 sched_len ints).
+// values), E (NT CB rows of NPHI + 2 values), X (NPHI padded slot blocks), the scaling rows (one opt_r
+// rot(dt/2) row, two rot(dt/2) rows, CB incoming amplitudes), the matrix rows (n_rot rows of NT + 4),
+// irot -> slot (n_rot ints), the slot sizes and first rows (2 NPHI ints), the schedule (8 sched_len ints).
 template <typename T>
 constexpr std::size_t pot5_smem(int n_rot, int nphi, int nt, int cb, int sched_len) {
   return 32 + sizeof(Vec<T>) * (static_cast<std::size_t>(cb) * (n_rot + 2) +
                                 static_cast<std::size_t>(nt) * cb * (nphi + 2) +
-                                static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb)) +
+                                static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb) +
+                                3 * static_cast<std::size_t>(n_rot) + cb) +
          sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) +
-         sizeof(int) * (static_cast<std::size_t>(n_rot) + 8 * sched_len);
+         sizeof(int) * (static_cast<std::size_t>(n_rot) + 2 * nphi + 8 * sched_len);
 }
 
 template <typename T, int NPHI, int NT, int CB>
@@ -122,9 +127,14 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   V* const F = reinterpret_cast<V*>(smem_raw + 32);  // [c][irot], columns of FCS values
   V* E = F + CB * FCS;                     // [line][phi], line = thread
   V* X = E + NTH * ERS;                    // [p][theta][c], slot blocks of SS values
-  T* L = reinterpret_cast<T*>(X + NPHI * SS);  // [irot][position of theta], rows of LDL
+  V* Bf = X + NPHI * SS;                   // [irot]: opt_r rot(dt/2) at the item's r point
+  V* R = Bf + n_rot;                       // [item parity][irot]: rot(dt/2) at the item's r point
+  V* SP = R + 2 * n_rot;                   // [c]: sp2sc(c) * chi, the item's incoming amplitudes
+  T* L = reinterpret_cast<T*>(SP + CB);    // [irot][position of theta], rows of LDL
   int* irot_slot = reinterpret_cast<int*>(L + n_rot * LDL);
-  int* sched = irot_slot + n_rot;
+  int* s_nj = irot_slot + n_rot;           // [slot]: J count
+  int* s_first = s_nj + NPHI;              // [slot]: first irot
+  int* sched = s_first + NPHI;
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int k = 0; k < 2; ++k) pot5::mbar_init(bars + k, NTH);
@@ -132,6 +142,10 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   }
   for (int k = tid; k < n_rot * LDL; k += NTH) L[k] = g.leg_rows[k];
   for (int k = tid; k < n_rot; k += NTH) irot_slot[k] = g.irot_slot[k];
+  for (int k = tid; k < NPHI; k += NTH) {
+    s_nj[k] = g.slot_nj[k];
+    s_first[k] = g.slot_nj[k] > 0 ? g.slot_first[k] : 0;
+  }
   for (int k = tid; k < 8 * g.sched_len; k += NTH) sched[k] = g.fwd_sched[k];
   __syncthreads();
 
@@ -143,6 +157,10 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   const int i0 = a.initial_channel;
   const uint32_t col_bytes = static_cast<uint32_t>(n_rot * sizeof(V));
   constexpr uint32_t row_bytes = NPHI * sizeof(V);
+  // The item's opt_z value, incoming amplitude chi(point) and (threads c < CB) sp2sc(column c), loaded
+  // when the item's copies are issued and used in its scaling phase.
+  T oz = 0;
+  V chi_in = cmake<V>(0, 0), sp_in = cmake<V>(0, 0);
 
   auto item_columns = [&](long long item, int& izr, int& c0, int& ncol) {
     izr = static_cast<int>(item / g.chunks);
@@ -150,17 +168,30 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     ncol = min(CB, a.n_xy - c0);
   };
   // Every thread arrives on each barrier once per phase; the threads that copy announce their bytes.
-  auto issue_psi = [&](long long item) {
+  // Threads c < ncol copy column c; thread CB the opt_r rot(dt/2) row, thread CB + 1 the rot(dt/2) row
+  // (into R[parity]).
+  auto issue_psi = [&](long long item, int parity_r) {
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
+    const int ir = izr % a.nr;
     if (tid < ncol) {
       pot5::fence_proxy_async();
       pot5::mbar_arrive_tx(bars, col_bytes);
       pot5::bulk_copy(F + tid * FCS, a.psi + (static_cast<long long>(izr) * a.n_xy + c0 + tid) * n_rot, col_bytes,
                       bars);
+    } else if (tid == CB || tid == CB + 1) {
+      pot5::fence_proxy_async();
+      pot5::mbar_arrive_tx(bars, col_bytes);
+      if (tid == CB)
+        pot5::bulk_copy(Bf, a.before + static_cast<long long>(ir) * n_rot, col_bytes, bars);
+      else
+        pot5::bulk_copy(R + parity_r * n_rot, a.rot_half + static_cast<long long>(ir) * n_rot, col_bytes, bars);
     } else {
       pot5::mbar_arrive(bars);
     }
+    oz = a.opt_z[izr / a.nr];
+    chi_in = a.chi[izr];
+    if (tid < ncol) sp_in = a.sp2sc[c0 + tid];
   };
   auto issue_exp = [&](long long item) {
     int izr, c0, ncol;
@@ -191,20 +222,21 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   };
 
   long long item = blockIdx.x;
+  int rp = 0;  // parity of the item count: the R row the current item reads
   if (item < g.n_items) {
-    issue_psi(item);
+    issue_psi(item, rp);
     issue_exp(item);
     pending = 3u;
   }
-  for (; item < g.n_items; item += gridDim.x) {
+  for (; item < g.n_items; item += gridDim.x, rp ^= 1) {
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
-    const int ir = izr % a.nr;
-    const int iz = izr / a.nr;
-    const T oz = a.opt_z[iz];
     const long long col_base = static_cast<long long>(izr) * a.n_xy + c0;
+    const V* rh_row = R + rp * n_rot;
+    if (tid < CB) SP[tid] = cmul(sp_in, chi_in);  // the previous item's scaling phase has read SP
 
-    // ---- wait for the columns, scale them in place (absorbers, rot(dt/2), the specular wave)
+    // ---- wait for the columns and rows, scale the columns in place (absorbers, rot(dt/2), the
+    // specular wave into the initial channel)
     if (wait_failed(bars, parity & 1u)) {
       give_up();
       return;
@@ -212,7 +244,7 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     parity ^= 1u;
     pending &= ~1u;
     for (int irot = tid; irot < n_rot; irot += NTH) {
-      const V b = a.before[ir * n_rot + irot];
+      const V b = Bf[irot];
 #pragma unroll
       for (int c = 0; c < CB; ++c) {
         V v = cmake<V>(0, 0);
@@ -220,9 +252,8 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
         F[c * FCS + irot] = v;
       }
       if (irot == i0) {
-        const V incoming = a.chi[izr];
-        const V rot_i0 = a.rot_half[ir * n_rot + i0];
-        for (int c = 0; c < ncol; ++c) F[c * FCS + i0] = cadd(F[c * FCS + i0], cmul(rot_i0, cmul(a.sp2sc[c0 + c], incoming)));
+        const V rot_i0 = rh_row[i0];
+        for (int c = 0; c < ncol; ++c) F[c * FCS + i0] = cadd(F[c * FCS + i0], cmul(rot_i0, SP[c]));
       }
     }
     __syncthreads();
@@ -232,8 +263,8 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     for (int s = 0; s < g.sched_len; ++s) {
       const int slot = sched[fg * g.sched_len + s];
       if (slot < 0) continue;
-      const int nj = __ldg(g.slot_nj + slot);
-      const int first = nj > 0 ? __ldg(g.slot_first + slot) : 0;
+      const int nj = s_nj[slot];
+      const int first = s_first[slot];
       T acc[4][4];
 #pragma unroll
       for (int q = 0; q < 4; ++q)
@@ -263,7 +294,7 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     __syncthreads();
     // the next item's columns (every thread has finished reading F)
     if (next < g.n_items) {
-      issue_psi(next);
+      issue_psi(next, rp ^ 1);
       pending |= 1u;
     }
 
@@ -341,7 +372,7 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
       for (int u = 0; u < 2; ++u) {
         const int irot = u == 0 ? ia : ib;
         if (u == 1 && !has_b) break;
-        const V rh = a.rot_half[ir * n_rot + irot];
+        const V rh = rh_row[irot];
 #pragma unroll
         for (int c = 0; c < CB; ++c)
           if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, cmake<V>(acc[u][c][0], acc[u][c][1]));
