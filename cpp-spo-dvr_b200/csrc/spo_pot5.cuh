@@ -243,17 +243,35 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     }
     parity ^= 1u;
     pending &= ~1u;
-    for (int irot = tid; irot < n_rot; irot += NTH) {
-      const V b = Bf[irot];
+    // Two rotational states per pass, all their loads before the first store (the compiler cannot tell
+    // that the runtime-strided stores to F miss the later loads, and would otherwise serialise them).
+    {
+      const V rot_i0 = rh_row[i0];
+      for (int ia = tid; ia < n_rot; ia += 2 * NTH) {
+        const int ib = ia + NTH;
+        const bool has_b = ib < n_rot;
+        const int irs[2] = {ia, has_b ? ib : ia};
+        V b[2], v[2][CB];
 #pragma unroll
-      for (int c = 0; c < CB; ++c) {
-        V v = cmake<V>(0, 0);
-        if (c < ncol) v = cscale(cmul(b, F[c * FCS + irot]), oz);
-        F[c * FCS + irot] = v;
-      }
-      if (irot == i0) {
-        const V rot_i0 = rh_row[i0];
-        for (int c = 0; c < ncol; ++c) F[c * FCS + i0] = cadd(F[c * FCS + i0], cmul(rot_i0, SP[c]));
+        for (int u = 0; u < 2; ++u) {
+          b[u] = Bf[irs[u]];
+#pragma unroll
+          for (int c = 0; c < CB; ++c) v[u][c] = F[c * FCS + irs[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (u == 1 && !has_b) break;
+          const bool at_i0 = irs[u] == i0;
+#pragma unroll
+          for (int c = 0; c < CB; ++c) {
+            V w = cmake<V>(0, 0);
+            if (c < ncol) {
+              w = cscale(cmul(b[u], v[u][c]), oz);
+              if (at_i0) w = cadd(w, cmul(rot_i0, SP[c]));  // the specular wave into the initial channel
+            }
+            F[c * FCS + irs[u]] = w;
+          }
+        }
       }
     }
     __syncthreads();
