@@ -346,6 +346,7 @@ void launch_pot2(int nphi, const spo::Pot2Args<T>& a, unsigned blocks, std::size
     case 16: launch_pot2_phi<T, 16>(a, blocks, smem, stream); break;
     case 20: launch_pot2_phi<T, 20>(a, blocks, smem, stream); break;
     case 24: launch_pot2_phi<T, 24>(a, blocks, smem, stream); break;
+    case 28: launch_pot2_phi<T, 28>(a, blocks, smem, stream); break;
     case 30: launch_pot2_phi<T, 30>(a, blocks, smem, stream); break;
     case 32: launch_pot2_phi<T, 32>(a, blocks, smem, stream); break;
     default: break;
@@ -382,6 +383,7 @@ void launch_pot3(int nphi, const spo::Pot2Args<T>& a, dim3 grid, unsigned thread
     case 16: launch_pot3_phi<T, 16>(a, grid, threads, smem, stream); break;
     case 20: launch_pot3_phi<T, 20>(a, grid, threads, smem, stream); break;
     case 24: launch_pot3_phi<T, 24>(a, grid, threads, smem, stream); break;
+    case 28: launch_pot3_phi<T, 28>(a, grid, threads, smem, stream); break;
     case 30: launch_pot3_phi<T, 30>(a, grid, threads, smem, stream); break;
     case 32: launch_pot3_phi<T, 32>(a, grid, threads, smem, stream); break;
     default: break;
@@ -412,6 +414,8 @@ Pot5Kernel<T> pot5_kernel_for(int nphi, int nt) {
     return nullptr;
   } else {
     if (nt == 16 && nphi == 32) return spo::potential5_kernel<T, 32, 16, 8>;
+    if (nt == 16 && nphi == 28) return spo::potential5_kernel<T, 28, 16, 8>;  // JMax 13 (theta 14, padded)
+    if (nt == 16 && nphi == 24) return spo::potential5_kernel<T, 24, 16, 8>;  // JMax 11 (theta 12, padded)
     if (nt == 8 && nphi == 16) return spo::potential5_kernel<T, 16, 8, 16>;
     if (nt == 4 && nphi == 8) return spo::potential5_kernel<T, 8, 4, 32>;
     if (nt == 4 && nphi == 12) return spo::potential5_kernel<T, 12, 4, 32>;
@@ -421,7 +425,7 @@ Pot5Kernel<T> pot5_kernel_for(int nphi, int nt) {
 
 bool pot2_phi_supported(int nphi) {
   switch (nphi) {
-    case 6: case 8: case 10: case 12: case 16: case 20: case 24: case 30: case 32: return true;
+    case 6: case 8: case 10: case 12: case 16: case 20: case 24: case 28: case 30: case 32: return true;
     default: return false;
   }
 }
@@ -576,9 +580,12 @@ class Step final : public StepBase {
     const bool xy2 = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx);
     out += std::string(" xy=") + (xy2 ? std::string(persist_xy_ ? "xy2p<" : "xy2<") + std::to_string(s_.nx) + "," + lanes(tile_xy_, s_.nx > 8) + ">"
                                       : std::string("xy_pass(general)"));
-    if (pot_kind_ == 5)
-      out += " potential=potential5<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
-             ",cb=" + std::to_string(128 / s_.nt) + ",blocks=" + std::to_string(pot5_blocks_) + ">";
+    if (pot_kind_ == 5) {
+      const int nt_k = (s_.nt == 12 || s_.nt == 14) ? 16 : s_.nt;  // 12 and 14 run on the 16-row tile
+      out += " potential=potential5<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(nt_k) +
+             ",cb=" + std::to_string(128 / nt_k) + ",blocks=" + std::to_string(pot5_blocks_) + ">";
+      if (nt_k != s_.nt) out += "(theta " + std::to_string(s_.nt) + " padded)";
+    }
     else if (pot_kind_ == 4)
       out += " potential=potential4<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
              ",cb=" + std::to_string(128 / s_.nt) + ",blocks=" + std::to_string(pot4_blocks_) + ">";
@@ -1413,10 +1420,16 @@ class Step final : public StepBase {
         pot3_args_.jp = jp;
       }
     }
-    // The persistent potential kernel with register-tiled contractions (ntheta 4, 8, 16; nphi 8, 16, 32).
-    pot4_kernel_ = (pot2_cb_ > 0 && 2 * s.mj_max + 1 <= s.nphi) ? pot4_kernel_for<T>(s.nphi, s.nt) : nullptr;
-    if (pot4_kernel_) {
-      const int cb = 128 / s.nt;
+    // The persistent potential kernels with register-tiled contractions: potential4 (ntheta 4, 8, 16;
+    // nphi 8, 16, 32) and potential5 (mixed form; ntheta 12 and 14 run on its 16-row tile, the matrix
+    // rows of the missing theta zero and their phi lines skipped).
+    const bool pot45_ok = pot2_cb_ > 0 && 2 * s.mj_max + 1 <= s.nphi;
+    const int nt_k = (s.nt == 12 || s.nt == 14) ? 16 : s.nt;
+    pot4_kernel_ = pot45_ok ? pot4_kernel_for<T>(s.nphi, s.nt) : nullptr;
+    Pot5Kernel<T> pot5_candidate = pot45_ok && s.n_rot % 2 == 0 ? pot5_kernel_for<T>(s.nphi, nt_k) : nullptr;
+    pot5_kernel_ = nullptr;
+    if (pot4_kernel_ || pot5_candidate) {
+      const int cb = 128 / nt_k;
       // Forward schedule: the slots in (+m, -m) pairs (m = 0 with an empty slot), pairs dealt to the four
       // warps largest first, each to the least loaded warp; half-warp 2w takes the first of each pair
       // of warp w, half-warp 2w + 1 the second.
@@ -1457,60 +1470,57 @@ class Step final : public StepBase {
           sched[(2 * w) * len + k] = warp[w][k].a;
           sched[(2 * w + 1) * len + k] = warp[w][k].b;
         }
-      std::vector<double> rows(static_cast<std::size_t>(s.n_rot) * (s.nt + 4), 0.0);
+      std::vector<double> rows(static_cast<std::size_t>(s.n_rot) * (nt_k + 4), 0.0);
       std::vector<int> irot_slot(s.n_rot);
       for (int b = 0; b < s.n_blocks; ++b)
         for (int j = 0; j < size[b]; ++j) {
           irot_slot[first[b] + j] = slot[b];
-          for (int t = 0; t < s.nt; ++t) {
-            const int quads = s.nt / 4;  // theta t at the position where the forward tiles read it
+          for (int t = 0; t < s.nt; ++t) {  // theta t >= s.nt (padding) stays zero
+            const int quads = nt_k / 4;  // theta t at the position where the forward tiles read it
             const int pos = (t % quads) * 4 + t / quads;
-            rows[static_cast<std::size_t>(first[b] + j) * (s.nt + 4) + pos] = legendre[offset[b] + t * size[b] + j];
+            rows[static_cast<std::size_t>(first[b] + j) * (nt_k + 4) + pos] = legendre[offset[b] + t * size[b] + j];
           }
         }
+      pot4_args_.p = pot2_.p;
+      pot4_args_.leg_rows = upload_real(rows);
+      pot4_args_.slot_first = upload_int(slot_first);
+      pot4_args_.slot_nj = upload_int(slot_nj);
+      pot4_args_.irot_slot = upload_int(irot_slot);
+      pot4_args_.fwd_sched = upload_int(sched);
+      pot4_args_.sched_len = len;
+      pot4_args_.chunks = static_cast<int>((nxy + cb - 1) / cb);
+      pot4_args_.n_items = static_cast<long long>(s.nzp) * s.nr * pot4_args_.chunks;
+      pot4_args_.identity_maps = pot2_.identity_maps;
+      pot4_args_.nt_table = s.nt;
+      int sms = 0;
+      check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
+      const long long items = std::max<long long>(pot4_args_.n_items, 1);
       pot4_smem_ = spo::pot4_smem<T>(s.n_rot, s.nphi, s.nt, cb, len);
-      // potential5: the same tables, the item data by bulk asynchronous copies (columns of n_rot values:
-      // 16-byte multiples when n_rot is even)
-      pot5_kernel_ = s.n_rot % 2 == 0 ? pot5_kernel_for<T>(s.nphi, s.nt) : nullptr;
-      pot5_smem_ = spo::pot5_smem<T>(s.n_rot, s.nphi, s.nt, cb, len);
-      if (pot5_kernel_ && pot5_smem_ <= static_cast<std::size_t>(smem_optin)) {
-        check_cuda(cudaFuncSetAttribute(pot5_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
-                   "potential5 smem");
-        int per_sm = 0, sms = 0;
-        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pot5_kernel_, 128, pot5_smem_),
-                   "potential5 occupancy");
-        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
-        pot5_blocks_per_sm_ = std::max(per_sm, 1);
-        pot5_sms_ = sms;
-        error_flag_ = dev<int>(1);
-        check_cuda(cudaMemset(error_flag_, 0, sizeof(int)), "error flag");
-      } else {
-        pot5_kernel_ = nullptr;
-      }
-      if (pot4_smem_ <= static_cast<std::size_t>(smem_optin)) {
+      if (pot4_kernel_ && pot4_smem_ <= static_cast<std::size_t>(smem_optin)) {
         check_cuda(cudaFuncSetAttribute(pot4_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
                    "potential4 smem");
-        int per_sm = 0, sms = 0;
+        int per_sm = 0;
         check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pot4_kernel_, 128, pot4_smem_),
                    "potential4 occupancy");
-        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
-        pot4_args_.p = pot2_.p;
-        pot4_args_.leg_rows = upload_real(rows);
-        pot4_args_.slot_first = upload_int(slot_first);
-        pot4_args_.slot_nj = upload_int(slot_nj);
-        pot4_args_.irot_slot = upload_int(irot_slot);
-        pot4_args_.fwd_sched = upload_int(sched);
-        pot4_args_.sched_len = len;
-        pot4_args_.chunks = static_cast<int>((nxy + cb - 1) / cb);
-        pot4_args_.n_items = static_cast<long long>(s.nzp) * s.nr * pot4_args_.chunks;
-        pot4_args_.identity_maps = pot2_.identity_maps;
-        pot4_blocks_ = static_cast<int>(std::min<long long>(static_cast<long long>(std::max(per_sm, 1)) * sms,
-                                                            std::max<long long>(pot4_args_.n_items, 1)));
-        pot5_blocks_ = static_cast<int>(std::min<long long>(static_cast<long long>(pot5_blocks_per_sm_) * pot5_sms_,
-                                                            std::max<long long>(pot4_args_.n_items, 1)));
+        pot4_blocks_ = static_cast<int>(std::min<long long>(static_cast<long long>(std::max(per_sm, 1)) * sms, items));
       } else {
         pot4_kernel_ = nullptr;
-        pot5_kernel_ = nullptr;
+      }
+      // potential5: the same tables, the item data by bulk asynchronous copies (columns of n_rot values:
+      // 16-byte multiples when n_rot is even)
+      pot5_smem_ = spo::pot5_smem<T>(s.n_rot, s.nphi, nt_k, cb, len);
+      if (pot5_candidate && pot5_smem_ <= static_cast<std::size_t>(smem_optin)) {
+        pot5_kernel_ = pot5_candidate;
+        check_cuda(cudaFuncSetAttribute(pot5_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
+                   "potential5 smem");
+        int per_sm = 0;
+        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pot5_kernel_, 128, pot5_smem_),
+                   "potential5 occupancy");
+        pot5_blocks_per_sm_ = std::max(per_sm, 1);
+        pot5_sms_ = sms;
+        pot5_blocks_ = static_cast<int>(std::min<long long>(static_cast<long long>(pot5_blocks_per_sm_) * sms, items));
+        error_flag_ = dev<int>(1);
+        check_cuda(cudaMemset(error_flag_, 0, sizeof(int)), "error flag");
       }
     }
     if (pot3_cb_ > 0 || pot4_kernel_ || pot5_kernel_) {

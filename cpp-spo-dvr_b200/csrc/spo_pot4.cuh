@@ -40,6 +40,8 @@ struct Pot4Args {
   int chunks;                // column chunks per point
   long long n_items;         // nz_potential * nr * chunks
   int identity_maps;
+  int nt_table;              // theta points of the exp(i A) table (potential5: NT, or fewer with the rest
+                             // of the tile padding)
 };
 
 // 4 consecutive real values (16-byte aligned) and 2 consecutive complex values.

@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   const int fg = tid / 16;
   const int line_c = tid % CB;
   const int line_t = tid / CB;
+  const int nt_table = g.nt_table;
   const int i0 = a.initial_channel;
   const uint32_t col_bytes = static_cast<uint32_t>(n_rot * sizeof(V));
   constexpr uint32_t row_bytes = NPHI * sizeof(V);
@@ -196,12 +197,12 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   auto issue_exp = [&](long long item) {
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
-    if (line_c < ncol) {
+    if (line_c < ncol && line_t < nt_table) {
       const int ixy = c0 + line_c;
       const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
       pot5::fence_proxy_async();
       pot5::mbar_arrive_tx(bars + 1, row_bytes);
-      pot5::bulk_copy(E + tid * ERS, a.expia + ((static_cast<long long>(izr) * a.n_rep + rep) * NT + line_t) * NPHI,
+      pot5::bulk_copy(E + tid * ERS, a.expia + ((static_cast<long long>(izr) * a.n_rep + rep) * nt_table + line_t) * NPHI,
                       row_bytes, bars + 1);
     } else {
       pot5::mbar_arrive(bars + 1);
@@ -323,7 +324,7 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     }
     parity ^= 2u;
     pending &= ~2u;
-    if (line_c < ncol) {
+    if (line_c < ncol && line_t < nt_table) {  // padding lines (theta >= nt_table) hold zeros
       const int ixy = c0 + line_c;
       V* xl = X + line_t * CB + line_c;
       const V* el = E + tid * ERS;

@@ -273,3 +273,40 @@ def test_balanced_axis_kernel_agrees(nz, nr, precision, monkeypatch):
         be.close()
     tol = 1e-13 if precision == "fp64" else 2e-6
     assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol
+
+
+@pytest.mark.parametrize("j_max", [11, 13])
+def test_potential5_pads_theta_12_and_14(j_max):
+    """The angular grids of the ensemble workload, theta 12 x phi 24 (JMax 11) and theta 14 x phi 28
+    (JMax 13), on potential5's 16-row tile (zero matrix rows for the missing theta, whose phi lines are
+    skipped), and potential2/3 with phi 28, against the general kernels: the potential stage to 2e-6,
+    an analysis step to 2e-5."""
+    from spo_b200 import capi, workload
+    case = workload.config_case({"nz": 32, "nr": 24, "nx": 4, "ny": 4, "j_max": j_max, "mj_max": j_max,
+                                 "nz_specular": 64, "nz_potential": 20})
+    assert case.m["n_theta"] == j_max + 1 and case.m["n_phi"] == 2 * j_max + 2
+    rng = np.random.default_rng(17)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    ref = make(case, "v1", "mixed")
+    ref.read_wave_packet(psi0, chi0)
+    ref.apply_stage(capi.STAGE_POTENTIAL)
+    p_stage, c_stage = ref.wave_packet_on_host()
+    ref.read_wave_packet(psi0, chi0)
+    ref.propagate_analysis_step()
+    p_step, c_step = ref.wave_packet_on_host()
+    ref.close()
+    for kernels in ("v2", "v3", "v5"):
+        be = make(case, kernels, "mixed")
+        assert f"potential=potential{kernels[1]}" in be.describe(), be.describe()
+        if kernels == "v5":
+            assert f"(theta {j_max + 1} padded)" in be.describe(), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.apply_stage(capi.STAGE_POTENTIAL)
+        p, c = be.wave_packet_on_host()
+        assert rel_err(p, p_stage) < 2e-6 and rel_err(c, c_stage) < 2e-6, kernels
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        p, c = be.wave_packet_on_host()
+        assert rel_l2(p, p_step) < 2e-5 and rel_l2(c, c_step) < 2e-5, kernels
+        be.close()
