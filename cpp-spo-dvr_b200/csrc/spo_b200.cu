@@ -978,7 +978,7 @@ class Step final : public StepBase {
   // with more than 8 sub-rows per line, by timing each on the zero wave packet the handle starts with
   // (a kinetic pass maps zero to zero, so the state is unchanged). All widths compute every line with the
   // same operations in the same order: the choice changes the speed, never the result.
-  // SPO_B200_TILES=8|16|32 fixes the choice; SPO_B200_AUTOTUNE=0 keeps the default (16).
+  // SPO_B200_TILES=8|16|32 (every pass) or z,r,xy fixes the choice; SPO_B200_AUTOTUNE=0 keeps the default (16).
   void autotune() {
     tile_z_ = tile_r_ = tile_xy_ = 0;
     zr_window_ = 0;
@@ -996,10 +996,20 @@ class Step final : public StepBase {
     balanced_ = use_v2_;
     tiles_source_ = "default";
     if (!use_v2_) return;
-    if (const char* env = std::getenv("SPO_B200_TILES")) {
-      const std::string t(env);
-      require(t == "8" || t == "16" || t == "32", "SPO_B200_TILES must be 8, 16 or 32");
-      tile_z_ = tile_r_ = tile_xy_ = std::stoi(t);
+    if (const char* env = std::getenv("SPO_B200_TILES")) {  // one width for every pass, or "z,r,xy"
+      std::vector<int> w;
+      std::string t(env);
+      for (std::size_t k = 0; k <= t.size();) {
+        const std::size_t e = std::min(t.find(',', k), t.size());
+        const std::string one = t.substr(k, e - k);
+        require(one == "8" || one == "16" || one == "32", "SPO_B200_TILES must be 8, 16 or 32, or three of them: z,r,xy");
+        w.push_back(std::stoi(one));
+        k = e + 1;
+      }
+      require(w.size() == 1 || w.size() == 3, "SPO_B200_TILES must be 8, 16 or 32, or three of them: z,r,xy");
+      tile_z_ = w[0];
+      tile_r_ = w.size() == 3 ? w[1] : w[0];
+      tile_xy_ = w.size() == 3 ? w[2] : w[0];
       tiles_source_ = "fixed";
     }
     if (const char* env = std::getenv("SPO_B200_ZR_WINDOW")) {  // lanes per Z+r window (0: two full passes)
