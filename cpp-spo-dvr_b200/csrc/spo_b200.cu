@@ -409,10 +409,15 @@ Pot4Kernel<T> pot4_kernel_for(int nphi, int nt) {
 template <typename T>
 using Pot5Kernel = void (*)(spo::Pot4Args<T>, int*);
 template <typename T>
-Pot5Kernel<T> pot5_kernel_for(int nphi, int nt) {
+Pot5Kernel<T> pot5_kernel_for(int nphi, int nt, bool l2e) {
   if constexpr (sizeof(T) != 4) {
     return nullptr;
   } else {
+    if (l2e) {
+      if (nt == 16 && nphi == 32) return spo::potential5_kernel<T, 32, 16, 8, true>;
+      if (nt == 16 && nphi == 28) return spo::potential5_kernel<T, 28, 16, 8, true>;
+      if (nt == 16 && nphi == 24) return spo::potential5_kernel<T, 24, 16, 8, true>;
+    }
     if (nt == 16 && nphi == 32) return spo::potential5_kernel<T, 32, 16, 8>;
     if (nt == 16 && nphi == 28) return spo::potential5_kernel<T, 28, 16, 8>;  // JMax 13 (theta 14, padded)
     if (nt == 16 && nphi == 24) return spo::potential5_kernel<T, 24, 16, 8>;  // JMax 11 (theta 12, padded)
@@ -583,7 +588,7 @@ class Step final : public StepBase {
     if (pot_kind_ == 5) {
       const int nt_k = (s_.nt == 12 || s_.nt == 14) ? 16 : s_.nt;  // 12 and 14 run on the 16-row tile
       out += " potential=potential5<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(nt_k) +
-             ",cb=" + std::to_string(128 / nt_k) + ",blocks=" + std::to_string(pot5_blocks_) + ">";
+             ",cb=" + std::to_string(128 / nt_k) + ",blocks=" + std::to_string(pot5_blocks_) + (pot5_l2e_ ? ",l2e" : "") + ">";
       if (nt_k != s_.nt) out += "(theta " + std::to_string(s_.nt) + " padded)";
     }
     else if (pot_kind_ == 4)
@@ -1436,7 +1441,8 @@ class Step final : public StepBase {
     const bool pot45_ok = pot2_cb_ > 0 && 2 * s.mj_max + 1 <= s.nphi;
     const int nt_k = (s.nt == 12 || s.nt == 14) ? 16 : s.nt;
     pot4_kernel_ = pot45_ok ? pot4_kernel_for<T>(s.nphi, s.nt) : nullptr;
-    Pot5Kernel<T> pot5_candidate = pot45_ok && s.n_rot % 2 == 0 ? pot5_kernel_for<T>(s.nphi, nt_k) : nullptr;
+    pot5_l2e_ = nt_k == 16 && !(std::getenv("SPO_B200_POT5_L2E") && std::string(std::getenv("SPO_B200_POT5_L2E")) == "0");
+    Pot5Kernel<T> pot5_candidate = pot45_ok && s.n_rot % 2 == 0 ? pot5_kernel_for<T>(s.nphi, nt_k, pot5_l2e_) : nullptr;
     pot5_kernel_ = nullptr;
     if (pot4_kernel_ || pot5_candidate) {
       const int cb = 128 / nt_k;
@@ -1518,11 +1524,13 @@ class Step final : public StepBase {
       }
       // potential5: the same tables, the item data by bulk asynchronous copies (columns of n_rot values:
       // 16-byte multiples when n_rot is even)
-      pot5_smem_ = spo::pot5_smem<T>(s.n_rot, s.nphi, nt_k, cb, len);
+      pot5_smem_ = spo::pot5_smem<T>(s.n_rot, s.nphi, nt_k, cb, len, pot5_l2e_);
       if (pot5_candidate && pot5_smem_ <= static_cast<std::size_t>(smem_optin)) {
         pot5_kernel_ = pot5_candidate;
         check_cuda(cudaFuncSetAttribute(pot5_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
                    "potential5 smem");
+        check_cuda(cudaFuncSetAttribute(pot5_kernel_, cudaFuncAttributePreferredSharedMemoryCarveout, 100),
+                   "potential5 carveout");
         int per_sm = 0;
         check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pot5_kernel_, 128, pot5_smem_),
                    "potential5 occupancy");
@@ -1632,6 +1640,7 @@ class Step final : public StepBase {
   Pot5Kernel<T> pot5_kernel_ = nullptr;
   int pot5_blocks_ = 0, pot5_blocks_per_sm_ = 1, pot5_sms_ = 0;
   std::size_t pot5_smem_ = 0;
+  bool pot5_l2e_ = false;  // potential5's L2E form (exp(i A) rows through L2, three blocks per SM)
   int* error_flag_ = nullptr;  // set by a kernel whose bounded wait gave up
   int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4, 5 potential5
   std::string pot_source_ = "default";

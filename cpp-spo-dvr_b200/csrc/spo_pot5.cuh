@@ -81,6 +81,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // Orders this thread's earlier shared-memory accesses before later asynchronous-proxy writes to them.
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Asks for `bytes` (a multiple of 16, 16-byte aligned) of global memory to be brought into L2.
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to this CTA's
 // shared memory, completing `bytes` on the barrier.
 __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -97,18 +102,23 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
 // values), E (NT CB rows of NPHI + 2 values), X (NPHI padded slot blocks), the scaling rows (one opt_r
 // rot(dt/2) row, two rot(dt/2) rows, CB incoming amplitudes), the matrix rows (n_rot rows of NT + 4),
 // irot -> slot (n_rot ints), the slot sizes and first rows (2 NPHI ints), the schedule (8 sched_len ints).
+// The L2E form keeps neither E nor the opt_r rot(dt/2) row in shared memory.
 template <typename T>
-constexpr std::size_t pot5_smem(int n_rot, int nphi, int nt, int cb, int sched_len) {
+constexpr std::size_t pot5_smem(int n_rot, int nphi, int nt, int cb, int sched_len, bool l2e = false) {
   return 32 + sizeof(Vec<T>) * (static_cast<std::size_t>(cb) * (n_rot + 2) +
-                                static_cast<std::size_t>(nt) * cb * (nphi + 2) +
+                                (l2e ? 0 : static_cast<std::size_t>(nt) * cb * (nphi + 2)) +
                                 static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb) +
-                                3 * static_cast<std::size_t>(n_rot) + cb) +
+                                (l2e ? 2 : 3) * static_cast<std::size_t>(n_rot) + cb) +
          sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) +
          sizeof(int) * (static_cast<std::size_t>(n_rot) + 2 * nphi + 8 * sched_len);
 }
 
-template <typename T, int NPHI, int NT, int CB>
-__global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, int* __restrict__ error_flag) {
+// L2E: the exp(i A) rows are not staged in shared memory; each item's block of them is prefetched into
+// L2 one item ahead (cp.async.bulk.prefetch.L2) and every thread reads its row from there at the start of
+// its phi phase, and the opt_r rot(dt/2) values of a thread's rotational states come one item ahead into
+// registers. That leaves ~75 KB of shared memory per block: three blocks (12 warps) per SM instead of two.
+template <typename T, int NPHI, int NT, int CB, bool L2E = false>
+__global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Args<T> g, int* __restrict__ error_flag) {
   using V = Vec<T>;
   static_assert(sizeof(T) == 4, "the mixed form");
   static_assert(NT * CB == 128 && NT % 4 == 0 && CB % 2 == 0, "tile shape");
@@ -125,10 +135,10 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // 0: F, 1: E
   V* const F = reinterpret_cast<V*>(smem_raw + 32);  // [c][irot], columns of FCS values
-  V* E = F + CB * FCS;                     // [line][phi], line = thread
-  V* X = E + NTH * ERS;                    // [p][theta][c], slot blocks of SS values
-  V* Bf = X + NPHI * SS;                   // [irot]: opt_r rot(dt/2) at the item's r point
-  V* R = Bf + n_rot;                       // [item parity][irot]: rot(dt/2) at the item's r point
+  V* E = F + CB * FCS;                     // [line][phi], line = thread (not with L2E)
+  V* X = E + (L2E ? 0 : NTH * ERS);        // [p][theta][c], slot blocks of SS values
+  V* Bf = X + NPHI * SS;                   // [irot]: opt_r rot(dt/2) at the item's r point (not with L2E)
+  V* R = Bf + (L2E ? 0 : n_rot);           // [item parity][irot]: rot(dt/2) at the item's r point
   V* SP = R + 2 * n_rot;                   // [c]: sp2sc(c) * chi, the item's incoming amplitudes
   T* L = reinterpret_cast<T*>(SP + CB);    // [irot][position of theta], rows of LDL
   int* irot_slot = reinterpret_cast<int*>(L + n_rot * LDL);
@@ -162,6 +172,7 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   // when the item's copies are issued and used in its scaling phase.
   T oz = 0;
   V chi_in = cmake<V>(0, 0), sp_in = cmake<V>(0, 0);
+  V bq[2] = {cmake<V>(0, 0), cmake<V>(0, 0)};  // L2E: opt_r rot(dt/2) of irot tid and tid + NTH
 
   auto item_columns = [&](long long item, int& izr, int& c0, int& ncol) {
     izr = static_cast<int>(item / g.chunks);
@@ -180,7 +191,7 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
       pot5::mbar_arrive_tx(bars, col_bytes);
       pot5::bulk_copy(F + tid * FCS, a.psi + (static_cast<long long>(izr) * a.n_xy + c0 + tid) * n_rot, col_bytes,
                       bars);
-    } else if (tid == CB || tid == CB + 1) {
+    } else if ((tid == CB && !L2E) || tid == CB + 1) {
       pot5::fence_proxy_async();
       pot5::mbar_arrive_tx(bars, col_bytes);
       if (tid == CB)
@@ -190,6 +201,11 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     } else {
       pot5::mbar_arrive(bars);
     }
+    if constexpr (L2E) {
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (tid + u * NTH < n_rot) bq[u] = a.before[static_cast<long long>(ir) * n_rot + tid + u * NTH];
+    }
     oz = a.opt_z[izr / a.nr];
     chi_in = a.chi[izr];
     if (tid < ncol) sp_in = a.sp2sc[c0 + tid];
@@ -197,6 +213,15 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   auto issue_exp = [&](long long item) {
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
+    if constexpr (L2E) {  // column tid's rows (nt_table NPHI contiguous values) into L2
+      if (tid < ncol) {
+        const int ixy = c0 + tid;
+        const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
+        pot5::prefetch_l2(a.expia + (static_cast<long long>(izr) * a.n_rep + rep) * nt_table * NPHI,
+                          static_cast<uint32_t>(nt_table * row_bytes));
+      }
+      return;
+    }
     if (line_c < ncol && line_t < nt_table) {
       const int ixy = c0 + line_c;
       const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
@@ -227,13 +252,14 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
   if (item < g.n_items) {
     issue_psi(item, rp);
     issue_exp(item);
-    pending = 3u;
+    pending = L2E ? 1u : 3u;
   }
   for (; item < g.n_items; item += gridDim.x, rp ^= 1) {
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
     const long long col_base = static_cast<long long>(izr) * a.n_xy + c0;
     const V* rh_row = R + rp * n_rot;
+    const int ir_item = izr % a.nr;
     if (tid < CB) SP[tid] = cmul(sp_in, chi_in);  // the previous item's scaling phase has read SP
 
     // ---- wait for the columns and rows, scale the columns in place (absorbers, rot(dt/2), the
@@ -255,7 +281,10 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
         V b[2], v[2][CB];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
-          b[u] = Bf[irs[u]];
+          if constexpr (L2E)
+            b[u] = ia == tid ? bq[u] : a.before[static_cast<long long>(ir_item) * n_rot + irs[u]];
+          else
+            b[u] = Bf[irs[u]];
 #pragma unroll
           for (int c = 0; c < CB; ++c) v[u][c] = F[c * FCS + irs[u]];
         }
@@ -318,6 +347,34 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
     }
 
     // ---- phi transform, exp(i A), inverse phi transform
+    if constexpr (L2E) {
+      if (line_c < ncol && line_t < nt_table) {  // padding lines (theta >= nt_table) hold zeros
+        const int ixy = c0 + line_c;
+        const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
+        const V* eg = a.expia + ((static_cast<long long>(izr) * a.n_rep + rep) * nt_table + line_t) * NPHI;
+        V* xl = X + line_t * CB + line_c;
+        V x[NPHI];
+        if (g.identity_maps) {
+          V e[NPHI];  // this line's row from L2, requested before the transform
+          static_for<0, NPHI / 2>([&](auto h) {
+            constexpr int P = 2 * SPO_CV(h);
+            const float4 q = __ldg(reinterpret_cast<const float4*>(eg + P));
+            e[P] = cmake<V>(q.x, q.y);
+            e[P + 1] = cmake<V>(q.z, q.w);
+          });
+          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
+          rdft<NPHI, +1>(x);
+          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(e[SPO_CV(p)], x[SPO_CV(p)]); });
+        } else {
+          const int* map = a.phi_map + ixy * NPHI;
+          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
+          rdft<NPHI, +1>(x);
+          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(eg[__ldg(map + SPO_CV(p))], x[SPO_CV(p)]); });
+        }
+        rdft<NPHI, -1>(x);
+        static_for<0, NPHI>([&](auto p) { xl[SPO_CV(p) * SS] = x[SPO_CV(p)]; });
+      }
+    } else {
     if (wait_failed(bars + 1, parity >> 1 & 1u)) {
       give_up();
       return;
@@ -346,11 +403,12 @@ __global__ void __launch_bounds__(NT * CB, 2) potential5_kernel(Pot4Args<T> g, i
       rdft<NPHI, -1>(x);
       static_for<0, NPHI>([&](auto p) { xl[SPO_CV(p) * SS] = x[SPO_CV(p)]; });
     }
+    }
     __syncthreads();
     // the next item's exp(i A) rows (every thread has read its row of this item)
     if (next < g.n_items) {
       issue_exp(next);
-      pending |= 2u;
+      if (!L2E) pending |= 2u;
     }
 
     // ---- transposed theta contraction, rot(dt/2), store: two rotational states per pass (irot and
