@@ -213,8 +213,10 @@ struct Axis2Args {
 };
 
 // Dynamic shared memory: (N TB + 2 N) values (axis2_smem).
+// Mixed form with at most 8 sub-rows: registers capped for 1536 threads per SM (r = 48 = 6 x 8 at 40
+// registers: six blocks of 256 threads instead of five, 1.23 -> 1.12 ms on configuration 3).
 template <typename T, int N1, int N2, int TB>
-__global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2_kernel(Axis2Args<T> a) {
+__global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2), sizeof(T) == 4 && (N1 > N2 ? N1 : N2) <= 8 ? 1536 / (TB*(N1 > N2 ? N1 : N2)) : 1) axis2_kernel(Axis2Args<T> a) {
   using V = Vec<T>;
   constexpr int N = N1 * N2;
   constexpr int NS = N1 > N2 ? N1 : N2;
