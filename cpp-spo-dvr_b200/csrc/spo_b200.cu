@@ -1891,7 +1891,10 @@ int spo_averages(spo_handle* h, const double* z, const double* z_specular, const
 // ---------------------------------------------------------------------------------------------
 // Ensembles: one analysis step of several handles captured as one CUDA graph, one branch per member
 // between a fork and a join, so that one graph launch runs every member's kernel sequence and the
-// independent members overlap on the GPU.
+// independent members overlap on the GPU. Members whose every pass fills the GPU on its own (256 MiB
+// or more of device memory) gain nothing from overlapping and lose L2 locality to it: their branches
+// are chained one after another inside the graph (32 members of the configuration-4 sizes: 8.81e10
+// grid-point-steps/s chained, 8.45e10 all overlapped).
 // ---------------------------------------------------------------------------------------------
 struct spo_ensemble {
   std::string err;
@@ -1948,9 +1951,14 @@ int spo_ensemble_create(spo_handle* const* members, int n_members, spo_ensemble*
     check_cuda(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
     capturing = true;
     check_cuda(cudaEventRecord(events[0], e->stream), "cudaEventRecord");
+    unsigned long long fills_gpu = 256ull << 20;  // SPO_B200_ENSEMBLE_CHAIN_BYTES overrides it
+    if (const char* env = std::getenv("SPO_B200_ENSEMBLE_CHAIN_BYTES")) fills_gpu = std::stoull(env);
+    cudaEvent_t chain = events[0];  // the last large member's end
     for (int i = 0; i < n_members; ++i) {
       StepBase& m = *e->members[i]->impl;
-      check_cuda(cudaStreamWaitEvent(branch[i], events[0], 0), "cudaStreamWaitEvent");
+      const bool large = m.bytes() >= fills_gpu;
+      check_cuda(cudaStreamWaitEvent(branch[i], large ? chain : events[0], 0), "cudaStreamWaitEvent");
+      if (large) chain = events[i + 1];
       m.set_stream(branch[i]);
       m.enqueue_analysis_step();
       m.set_stream(nullptr);

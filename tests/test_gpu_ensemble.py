@@ -26,8 +26,16 @@ def random_state(case, seed):
     return psi, chi
 
 
-def test_ensemble_steps_equal_each_member_alone():
+@pytest.mark.parametrize("chain", ["overlapped", "chained"])
+def test_ensemble_steps_equal_each_member_alone(chain, monkeypatch):
+    """Both graph shapes: members overlapped between the fork and the join (small members), and chained one
+    after another (members that fill the GPU; forced here by a zero size threshold)."""
     from spo_b200 import B200Backend, Ensemble, workload
+
+    if chain == "chained":
+        monkeypatch.setenv("SPO_B200_ENSEMBLE_CHAIN_BYTES", "0")
+    else:
+        monkeypatch.delenv("SPO_B200_ENSEMBLE_CHAIN_BYTES", raising=False)
 
     cases = [workload.config_case(cfg) for cfg, _ in MEMBERS]
     states = [random_state(c, 100 + i) for i, c in enumerate(cases)]
