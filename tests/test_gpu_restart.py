@@ -101,3 +101,38 @@ def test_b200_continues_a_checkpoint_of_the_reference_cpu_backend(tmp_path):
     psi_full, psi = wave_packet(full), wave_packet(second)
     assert psi.shape == psi_full.shape and psi.size > 100000
     assert float(np.linalg.norm(psi - psi_full) / np.linalg.norm(psi_full)) <= 1e-10
+
+
+FINE_ANALYSIS_FILES = ["fine_analysis/grid.json", "fine_analysis/scattering_summary.tsv", "fine_analysis/s_matrix.tsv",
+                       "fine_analysis/probabilities_rovib.tsv", "fine_analysis/probabilities_diffraction.tsv",
+                       "fine_analysis/spectrum/scattering_summary.tsv",
+                       "fine_analysis/spectrum/probabilities_rovib.tsv",
+                       "fine_analysis/spectrum/probabilities_diffraction.tsv"]
+
+
+def fine_input(t_start, t_end):
+    """The reference's fine-analysis runs (tests/test_restart.cpp:139-183): dtStep = dtAna = 10 au, 0 .. 600 au
+    (60 BK records; the values are not physical, the runs are only compared with each other)."""
+    cfg = base_input()
+    cfg.update({"dtStep": 10.0, "dtAna": 10.0, "dtAve": 100.0, "alsoAnalysis": True})
+    return with_times(cfg, t_start, t_end, int((t_end - t_start) / 10.0 + 0.5))
+
+
+def test_fine_analysis_of_b200_bk_files_is_the_same_in_every_run_mode(tmp_path):
+    """The fine analysis (§8(f)4: the reference's host post-processing of the BK file) of BK coefficients that
+    the B200 computed: alsoAnalysis after the run, the same run split by a restart, and onlyAnalysis of the
+    native and of the Fortran BK file give bitwise the same files (as tests/test_restart.cpp:204-219)."""
+    full = run(fine_input(0.0, 600.0), tmp_path / "full", "b200")
+    first = run(fine_input(0.0, 300.0), tmp_path / "first", "b200")
+    second = run(restart_from(fine_input(300.0, 600.0), first), tmp_path / "second", "b200")
+    outs = {"second": second}
+    for fmt in ("native", "fortran"):
+        cfg = fine_input(0.0, 600.0)
+        cfg.update({"alsoAnalysis": False, "onlyAnalysis": True, "RestartDir": str(full), "RestartFormat": fmt})
+        outs[fmt] = run(cfg, tmp_path / f"only_{fmt}", "b200")
+    assert (full / "fine_analysis" / "s_matrix.tsv").exists()
+    for name in FINE_ANALYSIS_FILES:
+        ref = (full / name).read_bytes()
+        assert ref, name
+        for other, out in outs.items():
+            assert (out / name).read_bytes() == ref, (other, name)
