@@ -603,7 +603,7 @@ __global__ void bk_specular_kernel(const Vec<T>* __restrict__ chi, int nr, int i
 }
 
 // S-matrix sums (s_matrix.cpp:49-56): sums(k, ien) += bk(k) exp(i E_ien t) dt_analysis, FP64.
-__global__ void s_matrix_add_kernel(const double2* __restrict__ bk, int n, const double* __restrict__ energies,
+static __global__ void s_matrix_add_kernel(const double2* __restrict__ bk, int n, const double* __restrict__ energies,
                                     int n_energies, double time, double dt, double2* __restrict__ sums) {
   const long long total = static_cast<long long>(n) * n_energies;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;

@@ -283,8 +283,12 @@ int spo_ensemble_destroy(spo_ensemble* e);
  * every GPU which loads the library holds until the process exits. All calls share that array: calls
  * that overlap on the GPU (different streams or threads at the same time) race on it. Every element a
  * call reads is written by the same call first, so nothing needs clearing between calls. The first
- * call on a device looks up the array's device address for that device, with it current; make that
- * first call before any stream capture. Messages of refused calls: spo_last_error(NULL).
+ * call on a device looks up the array's device address for that device, with it current; only a
+ * successful lookup is kept, so a lookup that failed (for example while memory was exhausted) is tried
+ * again by the next call. The call synchronises the stream and copies into pageable host memory, so it
+ * cannot run on a capturing stream: it refuses one with SPO_ERR_STATE. A CUDA error left pending by
+ * earlier work on the calling thread is reported as such (SPO_ERR_DEVICE) and left pending.
+ * Messages of refused calls: spo_last_error(NULL).
  * --------------------------------------------------------------------------------------------- */
 #define SPO_NOALLOC_MAX_BLOCKS 65536
 int spo_block_densities_noalloc(const void* psi_device, int precision, long long n_blocks, long long block_size,

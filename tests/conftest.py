@@ -30,12 +30,16 @@ def pytest_configure(config):
 
 def _ensure_built():
     """Builds the oracle and the product library when they are missing and their sources exist."""
-    if not os.path.exists(REF_TOOL) and os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "all"], check=True,
-                       stdout=subprocess.DEVNULL)
+    reference = os.environ.get("SPODVR_REFERENCE")
+    if not os.path.exists(REF_TOOL):
+        if not reference or not os.path.isdir(reference):
+            pytest.fail(f"the oracle {REF_TOOL} is not built: run __graft_entry__.build(), or set SPODVR_REFERENCE "
+                        "to the reference checkout and run make -C oracle")
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "all", f"SPODVR_REFERENCE={reference}"],
+                       check=True, stdout=subprocess.DEVNULL)
     lib = os.path.join(ROOT, "cpp-spo-dvr_b200", "lib", "libspo_b200.so")
     if not os.path.exists(lib):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "cpp-spo-dvr_b200")], check=True, stdout=subprocess.DEVNULL)
+        subprocess.run(["make", "-C", os.path.join(ROOT, "cpp-spo-dvr_b200"), "-j4"], check=True, stdout=subprocess.DEVNULL)
 
 
 @pytest.fixture(scope="session")

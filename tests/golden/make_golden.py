@@ -1,7 +1,8 @@
 """Writes the committed golden fixtures of tests/golden/ from the reference's own regression data.
 
-Run once in a checkout where the reference project is present (its path is the first argument,
-default /root/reference); the outputs are committed, so the tests never read the reference.
+Run once in a checkout where the reference project is present (its path is the first argument, else
+the SPODVR_REFERENCE environment variable); the outputs are committed, so the tests never read the
+reference.
 
 For each regression case of the reference (tests/reference/<case>/, Fortran outputs with their
 input.json), it writes tests/golden/<case>/:
@@ -37,7 +38,10 @@ def fortran_records(path):
     return out
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=None):
+    ref_root = ref_root or os.environ.get("SPODVR_REFERENCE")
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "tests", "reference")):
+        sys.exit("make_golden.py: give the reference checkout as the first argument or in SPODVR_REFERENCE")
     here = os.path.dirname(os.path.abspath(__file__))
     for case, stride in CASES.items():
         src = os.path.join(ref_root, "tests", "reference", case)

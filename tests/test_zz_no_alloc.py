@@ -76,3 +76,23 @@ def test_noalloc_refuses_sizes_beyond_its_limit():
                                          capi.NOALLOC_MAX_BLOCKS + 1, 1, capi.dptr(out), None)
     assert st == capi.SPO_ERR_INVALID
     assert "exceeds SPO_NOALLOC_MAX_BLOCKS" in lib.spo_last_error(None).decode()
+
+
+def test_noalloc_at_exactly_its_limit():
+    """n_blocks = SPO_NOALLOC_MAX_BLOCKS: the last element of the shared array and the full grid are used."""
+    import torch
+
+    from spo_b200 import capi
+
+    lib = capi.lib()
+    n_blocks, block_size = capi.NOALLOC_MAX_BLOCKS, 4
+    rng = np.random.default_rng(5)
+    psi = rng.standard_normal((n_blocks, block_size)) + 1j * rng.standard_normal((n_blocks, block_size))
+    psi[-1] *= 3.0  # a distinct last block
+    expected = np.sum(np.abs(psi) ** 2, axis=1)
+    tensor = torch.from_numpy(psi.reshape(-1)).cuda()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        got = noalloc_densities(lib, tensor, capi.PRECISION_FP64, n_blocks, block_size,
+                                torch.cuda.current_stream().cuda_stream)
+        assert np.max(np.abs(got - expected)) <= 1e-13 * np.max(expected)
