@@ -191,13 +191,39 @@ def cpu_sample_input(nx: int):
     return path
 
 
+def host_cpu():
+    """The host's CPU model, logical CPUs and physical cores (from /proc/cpuinfo)."""
+    model, cores = None, set()
+    phys = core = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            key, _, val = line.partition(":")
+            key, val = key.strip(), val.strip()
+            if key == "model name" and model is None:
+                model = val
+            elif key == "physical id":
+                phys = val
+            elif key == "core id":
+                core = val
+            elif not key and phys is not None and core is not None:
+                cores.add((phys, core))
+                phys = core = None
+        if phys is not None and core is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    logical = os.cpu_count() or 1
+    return {"model": model, "logical_cpus": logical, "physical_cores": len(cores) or logical}
+
+
 def reference_timing(analysis_steps: int, warmup: int, nx: int = 4):
-    """The reference CPU path (oracle/_ref) on all host threads: JSON of spo_ref_tool time."""
+    """The reference CPU path (oracle/_ref) on one thread per physical core: JSON of spo_ref_tool time."""
     if not os.path.exists(REF_TOOL):
         return None, f"{REF_TOOL} is not built"
     path = cpu_sample_input(nx)
     env = dict(os.environ)
-    env.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    cpu = host_cpu()
+    env.setdefault("OMP_NUM_THREADS", str(cpu["physical_cores"]))
     try:
         r = subprocess.run([REF_TOOL, "time", path, "--analysis-steps", str(analysis_steps), "--warmup", str(warmup)],
                            capture_output=True, text=True, env=env, timeout=1800)
@@ -206,10 +232,13 @@ def reference_timing(analysis_steps: int, warmup: int, nx: int = 4):
     if r.returncode != 0:
         return None, r.stderr.strip()[-300:]
     out = json.loads(r.stdout.strip().splitlines()[-1])
-    out["sample"] = (f"config-2 reference input (Dai-Light PES, HD, JMax = MJMax = 15) with nX = nY = {nx}: "
+    grid = "the full grid" if nx == 16 else f"nX = nY = {nx} ({nx * nx}/256 of the points)"
+    out["sample"] = (f"config-2 reference input (Dai-Light PES, HD, JMax = MJMax = 15) on {grid}: "
                      f"{int(out['n_points'])} 6D points, {analysis_steps} analysis steps of 5 time steps after "
                      f"{warmup} warm-up; reference CpuBackend compiled from its sources (FFT: the project's FP64 "
-                     f"substitute, FFTW being absent)")
+                     f"substitute, FFTW being absent); {out['threads']} OpenMP threads on "
+                     f"{cpu['physical_cores']} physical cores ({cpu['logical_cpus']} logical) of {cpu['model']}")
+    out["cpu"] = cpu
     return out, None
 
 

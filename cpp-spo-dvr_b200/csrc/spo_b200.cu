@@ -169,6 +169,14 @@ int spo_profile_entry(const spo_handle* h, int i, char* name, int name_len, doub
   return SPO_OK;
 }
 
+int spo_test_wait_timeout(spo_handle* h, int poll_limit, int unmatched_bytes) {
+  if (h && (unmatched_bytes < 0 || unmatched_bytes % 16 != 0 || unmatched_bytes > 4096)) {
+    h->err = "spo_test_wait_timeout: unmatched_bytes must be a multiple of 16 in [0, 4096]";
+    return SPO_ERR_INVALID;
+  }
+  return guarded(h, [&] { h->impl->set_wait_test(poll_limit, static_cast<unsigned>(unmatched_bytes)); });
+}
+
 int spo_device_bytes(const spo_handle* h, unsigned long long* bytes) {
   if (!h || !bytes) return SPO_ERR_INVALID;
   *bytes = h->impl->bytes();

@@ -33,6 +33,7 @@
 #include "spo_regfft.cuh"
 #include "spo_pot4.cuh"
 #include "spo_pot5.cuh"
+#include "spo_pot6.cuh"
 #include "spo_persist.cuh"
 
 namespace spo_host {
@@ -535,6 +536,7 @@ class StepBase {
   virtual int launches() const = 0;
   virtual void set_stream(cudaStream_t s) = 0;
   virtual void profile(bool on) = 0;
+  virtual void set_wait_test(int poll_limit, unsigned extra_bytes) = 0;
   virtual const std::vector<KernelRecord>& records() const = 0;
 };
 
@@ -554,6 +556,14 @@ class Step final : public StepBase {
     check_device_error();
   }
 
+  // Failure-detection test: the waits of potential5/6 give up after poll_limit polls (<= 0: the default),
+  // and every item's first barrier phase expects extra_bytes more than its copies deliver.
+  void set_wait_test(int poll_limit, unsigned extra_bytes) override {
+    const int limit = poll_limit > 0 ? poll_limit : spo::pot5::kWaitLimit;
+    pot4_args_.poll_limit = pot6_args_.poll_limit = limit;
+    pot4_args_.extra_tx = pot6_args_.extra_tx = extra_bytes;
+  }
+
   // A kernel whose bounded wait gave up has set the device flag: report it (and clear it).
   void check_device_error() {
     if (!error_flag_) return;
@@ -561,7 +571,8 @@ class Step final : public StepBase {
     check_cuda(cudaMemcpy(&flag, error_flag_, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
     if (flag) {
       check_cuda(cudaMemset(error_flag_, 0, sizeof(int)), "error flag");
-      throw SpoError(SPO_ERR_TIMEOUT, "potential5: a bounded wait for an asynchronous copy gave up");
+      throw SpoError(SPO_ERR_TIMEOUT, std::string(pot_kind_ == 6 ? "potential6" : "potential5") +
+                                          ": a bounded wait for an asynchronous copy or tensor-core work gave up");
     }
   }
 
@@ -589,7 +600,10 @@ class Step final : public StepBase {
     const bool xy2 = use_v2_ && s_.nx == s_.ny && xy2_supported(s_.nx);
     out += std::string(" xy=") + (xy2 ? std::string(persist_xy_ ? "xy2p<" : "xy2<") + std::to_string(s_.nx) + "," + lanes(tile_xy_, s_.nx > 8) + ">"
                                       : std::string("xy_pass(general)"));
-    if (pot_kind_ == 5) {
+    if (pot_kind_ == 6) {
+      out += " potential=potential6<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(s_.nt) +
+             ",tcgen05.tf32x3,tile=64,blocks=" + std::to_string(pot6_blocks_) + ">";
+    } else if (pot_kind_ == 5) {
       const int nt_k = (s_.nt == 12 || s_.nt == 14) ? 16 : s_.nt;  // 12 and 14 run on the 16-row tile
       out += " potential=potential5<nphi=" + std::to_string(s_.nphi) + ",nt=" + std::to_string(nt_k) +
              ",cb=" + std::to_string(128 / nt_k) + ",blocks=" + std::to_string(pot5_blocks_) + (pot5_l2e_ ? ",l2e" : "") + ">";
@@ -938,7 +952,9 @@ class Step final : public StepBase {
     const double bytes = sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia()));
     const unsigned points = static_cast<unsigned>(s_.nzp) * s_.nr;
     if (pot_kind_ >= 3) {
-      if (pot_kind_ == 5) {
+      if (pot_kind_ == 6) {
+        pot6_kernel_<<<pot6_blocks_, spo::kPot6Threads, pot6_smem_, stream_>>>(pot6_args_, error_flag_);
+      } else if (pot_kind_ == 5) {
         pot5_kernel_<<<pot5_blocks_, 128, pot5_smem_, stream_>>>(pot4_args_, error_flag_);
       } else if (pot_kind_ == 4) {
         pot4_kernel_<<<pot4_blocks_, 128, pot4_smem_, stream_>>>(pot4_args_);
@@ -1512,6 +1528,8 @@ class Step final : public StepBase {
       pot4_args_.n_items = static_cast<long long>(s.nzp) * s.nr * pot4_args_.chunks;
       pot4_args_.identity_maps = pot2_.identity_maps;
       pot4_args_.nt_table = s.nt;
+      pot4_args_.poll_limit = spo::pot5::kWaitLimit;
+      pot4_args_.extra_tx = 0;
       int sms = 0;
       check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
       const long long items = std::max<long long>(pot4_args_.n_items, 1);
@@ -1545,7 +1563,66 @@ class Step final : public StepBase {
         check_cuda(cudaMemset(error_flag_, 0, sizeof(int)), "error flag");
       }
     }
-    if (pot3_cb_ > 0 || pot4_kernel_ || pot5_kernel_) {
+    // potential6 (mixed form): both theta contractions as split-precision TF32 tcgen05 GEMMs over 64-column
+    // tiles, for the square heteronuclear basis JMax = MJMax = 15 with ntheta 16 and nphi 32 (configuration
+    // 2's angular grid); one block of 256 threads per SM holding all 512 tensor-memory columns.
+    pot6_kernel_ = nullptr;
+    if constexpr (std::is_same_v<T, float>) {
+      using B6 = spo::pot6::Basis<16>;
+      bool square = pot2_cb_ > 0 && s.nt == 16 && s.nphi == 32 && s.n_rot == B6::kRot && s.n_blocks == B6::kBlocks;
+      for (int b = 0; square && b < s.n_blocks; ++b) square = first[b] == B6::first(b) && size[b] == B6::nj(b);
+      const std::size_t need = spo::pot6_smem<16>();
+      if (square && need <= static_cast<std::size_t>(smem_optin)) {
+        auto tf32 = [](double v) {  // round to TF32 (nearest, ties away from zero), as cvt.rna.tf32.f32
+          const float f = static_cast<float>(v);
+          uint32_t u;
+          std::memcpy(&u, &f, 4);
+          u = (u + 0x1000u) & 0xFFFFE000u;
+          float r;
+          std::memcpy(&r, &u, 4);
+          return r;
+        };
+        // [forward hi | forward lo | transposed hi | transposed lo], canonical K-major layouts (core matrices
+        // of 8 rows x 4 values): forward block b: N = theta (16) x K = J (padded to 8 or 16); transposed:
+        // N = J (padded to 16) x K = theta (16).
+        std::vector<float> tabs(2 * static_cast<std::size_t>(B6::kBfFloats + B6::kBbFloats), 0.0f);
+        auto core = [](int n, int k) { return ((k / 4) * 2 + n / 8) * 32 + (n % 8) * 4 + k % 4; };
+        for (int b = 0; b < s.n_blocks; ++b)
+          for (int t = 0; t < 16; ++t)
+            for (int j = 0; j < size[b]; ++j) {
+              const double m = legendre[offset[b] + t * size[b] + j];
+              const float hi = tf32(m), lo = tf32(m - static_cast<double>(hi));
+              const std::size_t f = B6::bf_offset(b) + core(t, j);
+              tabs[f] = hi;
+              tabs[B6::kBfFloats + f] = lo;
+              const std::size_t r = 2 * static_cast<std::size_t>(B6::kBfFloats) + b * 256 + core(j, t);
+              tabs[r] = hi;
+              tabs[B6::kBbFloats + r] = lo;
+            }
+        float* dtabs = dev<float>(tabs.size());
+        check_cuda(cudaMemcpy(dtabs, tabs.data(), sizeof(float) * tabs.size(), cudaMemcpyHostToDevice), "potential6 tables");
+        pot6_args_.p = pot2_.p;
+        pot6_args_.bf = dtabs;
+        pot6_args_.bb = dtabs + 2 * B6::kBfFloats;
+        pot6_args_.tiles = static_cast<int>((nxy + spo::kPot6Tile - 1) / spo::kPot6Tile);
+        pot6_args_.n_items = static_cast<long long>(s.nzp) * s.nr * pot6_args_.tiles;
+        pot6_args_.identity_maps = pot2_.identity_maps;
+        pot6_args_.poll_limit = spo::pot5::kWaitLimit;
+        pot6_args_.extra_tx = 0;
+        pot6_kernel_ = spo::potential6_kernel<32, 16>;
+        pot6_smem_ = need;
+        check_cuda(cudaFuncSetAttribute(pot6_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(need)),
+                   "potential6 smem");
+        int sms = 0;
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id), "SM count");
+        pot6_blocks_ = static_cast<int>(std::min<long long>(sms, std::max<long long>(pot6_args_.n_items, 1)));
+        if (!error_flag_) {
+          error_flag_ = dev<int>(1);
+          check_cuda(cudaMemset(error_flag_, 0, sizeof(int)), "error flag");
+        }
+      }
+    }
+    if (pot3_cb_ > 0 || pot4_kernel_ || pot5_kernel_ || pot6_kernel_) {
       require(sizeof(V) * (nxy + 1) <= static_cast<std::size_t>(smem_optin), "nx*ny too large for the projection kernel");
       check_cuda(cudaFuncSetAttribute(spo::projection_finalize_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem_optin), "projection smem");
@@ -1558,17 +1635,20 @@ class Step final : public StepBase {
     if (use_v2_ && pot3_cb_ > 0) pot_kind_ = 3;
     if (use_v2_ && pot4_kernel_) pot_kind_ = 4;
     if (use_v2_ && pot5_kernel_) pot_kind_ = 5;
+    if (use_v2_ && pot6_kernel_) pot_kind_ = 6;
     pot_source_ = "default";
     if (const char* env = std::getenv("SPO_B200_KERNELS")) {
       const std::string k(env);
-      require(k == "v1" || k == "v2" || k == "v3" || k == "v4" || k == "v5",
-              "SPO_B200_KERNELS must be v1, v2, v3, v4 or v5");
+      require(k == "v1" || k == "v2" || k == "v3" || k == "v4" || k == "v5" || k == "v6",
+              "SPO_B200_KERNELS must be v1, v2, v3, v4, v5 or v6");
       use_v2_ = k != "v1";
       const int want = k[1] - '0';
       const bool have = want == 1 || (want == 2 && pot2_cb_ > 0) || (want == 3 && pot3_cb_ > 0) ||
-                        (want == 4 && pot4_kernel_ != nullptr) || (want == 5 && pot5_kernel_ != nullptr);
+                        (want == 4 && pot4_kernel_ != nullptr) || (want == 5 && pot5_kernel_ != nullptr) ||
+                        (want == 6 && pot6_kernel_ != nullptr);
       // an unavailable kernel falls back to the best available one below it
-      const bool avail[6] = {false, true, pot2_cb_ > 0, pot3_cb_ > 0, pot4_kernel_ != nullptr, pot5_kernel_ != nullptr};
+      const bool avail[7] = {false, true, pot2_cb_ > 0, pot3_cb_ > 0, pot4_kernel_ != nullptr, pot5_kernel_ != nullptr,
+                             pot6_kernel_ != nullptr};
       pot_kind_ = have ? want : 1;
       if (!have)
         for (int k = want - 1; k >= 2; --k)
@@ -1646,7 +1726,12 @@ class Step final : public StepBase {
   std::size_t pot5_smem_ = 0;
   bool pot5_l2e_ = false;  // potential5's L2E form (exp(i A) rows through L2, three blocks per SM)
   int* error_flag_ = nullptr;  // set by a kernel whose bounded wait gave up
-  int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4, 5 potential5
+  int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4, 5 potential5, 6 potential6
+  // potential6: both theta contractions on the tensor cores (mixed form, nphi 32, ntheta 16, square basis)
+  spo::Pot6Args<float> pot6_args_{};
+  void (*pot6_kernel_)(spo::Pot6Args<float>, int*) = nullptr;
+  int pot6_blocks_ = 0;
+  std::size_t pot6_smem_ = 0;
   std::string pot_source_ = "default";
   int tile_z_ = 0, tile_r_ = 0, tile_xy_ = 0;  // batch lanes per block of the register kinetic kernels (0: default)
   long long zr_window_ = 0;                     // lanes per Z+r window (0: two full passes)

@@ -200,7 +200,8 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(GemmArgs g) {
     }
     tc::fence_proxy_async();  // the generic writes, visible to the tensor core
   };
-  uint32_t parity = 0;  // bit s: the phase parity of stage s's barrier
+  uint32_t parity = 0;   // bit s: the phase parity of stage s's barrier
+  uint32_t pending = 0;  // bit s: a commit on stage s's barrier not yet waited for
   bool failed = false;
   if (kc_first < kc_last) stage(0, kc_first);
   tc::fence_before_sync();
@@ -219,12 +220,16 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(GemmArgs g) {
       }
       tc::commit(bar + st);
     }
+    pending |= 1u << st;
     if (kc + 1 < kc_last) {
       // the other stage's previous chunk (kc - 1) must be multiplied before it is overwritten
       bool ok = true;
       if (kc > kc_first) {
         ok = tc::mbar_wait(bar + (st ^ 1), parity >> (st ^ 1) & 1u);
-        parity ^= 1u << (st ^ 1);
+        if (ok) {
+          parity ^= 1u << (st ^ 1);
+          pending &= ~(1u << (st ^ 1));
+        }
       }
       if (__syncthreads_or(!ok)) {
         failed = true;
@@ -240,11 +245,15 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(GemmArgs g) {
   if (!failed && kc_last > kc_first) {
     const int last = (kc_last - kc_first - 1) & 1;
     const bool ok = tc::mbar_wait(bar + last, parity >> last & 1u);
+    if (ok) pending = 0;  // the last commit arrives after every earlier MMA of the issuing thread
     failed = __syncthreads_or(!ok) != 0;
   }
   tc::fence_after_sync();
   if (failed) {
     if (tid == 0) atomicExch(g.error_flag, 1);
+    // bounded waits for the MMAs in flight, so that none still writes the accumulator when it is freed
+    for (int k = 0; k < 2; ++k)
+      if (pending >> k & 1u) tc::mbar_wait(bar + k, parity >> k & 1u);
   } else if (kc_last > kc_first) {
     const int row = m0 + warp * 32 + lane;
     for (int j = 0; j < g.n / 16; ++j) {

@@ -42,6 +42,9 @@ struct Pot4Args {
   int identity_maps;
   int nt_table;              // theta points of the exp(i A) table (potential5: NT, or fewer with the rest
                              // of the tile padding)
+  int poll_limit;            // potential5: polls before a wait on an mbarrier gives up
+  unsigned extra_tx;         // potential5: bytes announced beyond those copied (0; a failure-detection test
+                             // sets it so that a barrier phase cannot complete and the wait gives up)
 };
 
 // 4 consecutive real values (16-byte aligned) and 2 consecutive complex values.

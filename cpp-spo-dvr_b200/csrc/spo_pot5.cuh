@@ -60,11 +60,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
       : "memory");
 }
 
-// Waits for the phase with the given parity to complete; false after kWaitLimit polls.
+// Waits for the phase with the given parity to complete; false after `limit` polls (kWaitLimit by default).
 constexpr int kWaitLimit = 1 << 22;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = kWaitLimit) {
   const uint32_t addr = smem_addr(bar);
-  for (int i = 0; i < kWaitLimit; ++i) {
+  for (int i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     const int ir = izr % a.nr;
     if (tid < ncol) {
       pot5::fence_proxy_async();
-      pot5::mbar_arrive_tx(bars, col_bytes);
+      pot5::mbar_arrive_tx(bars, col_bytes + (tid == 0 ? g.extra_tx : 0u));
       pot5::bulk_copy(F + tid * FCS, a.psi + (static_cast<long long>(izr) * a.n_xy + c0 + tid) * n_rot, col_bytes,
                       bars);
     } else if ((tid == CB && !L2E) || tid == CB + 1) {
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
   };
   // A bounded wait by every thread; true (for the whole block) when one of them gave up.
   auto wait_failed = [&](uint64_t* bar, uint32_t parity) {
-    const bool ok = pot5::mbar_wait(bar, parity);
+    const bool ok = pot5::mbar_wait(bar, parity, g.poll_limit);
     return __syncthreads_or(!ok) != 0;
   };
   // Phase parities (bit 0: F, bit 1: E) and copies issued but not yet waited for (same bits).
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     if (tid == 0) atomicExch(error_flag, 1);
     // bounded waits for this block's copies in flight, so that none lands after the block has left
     for (int k = 0; k < 2; ++k)
-      if (pending >> k & 1u) pot5::mbar_wait(bars + k, parity >> k & 1u);
+      if (pending >> k & 1u) pot5::mbar_wait(bars + k, parity >> k & 1u, g.poll_limit);
   };
 
   long long item = blockIdx.x;

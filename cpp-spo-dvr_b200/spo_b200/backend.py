@@ -194,6 +194,12 @@ class B200Backend:
         """Run on the caller's cudaStream_t (an integer handle, e.g. torch.cuda.Stream().cuda_stream)."""
         self._check(self._lib.spo_set_stream(self._h, ctypes.c_void_p(cuda_stream or 0)))
 
+    def test_wait_timeout(self, poll_limit: int, unmatched_bytes: int) -> None:
+        """Failure-detection test of the bounded device waits (spo_test_wait_timeout): the potential kernel's
+        barriers expect unmatched_bytes more than their copies deliver and give up after poll_limit polls;
+        (0, 0) restores normal operation."""
+        self._check(self._lib.spo_test_wait_timeout(self._h, poll_limit, unmatched_bytes))
+
     def profile(self, enable: bool) -> None:
         self._check(self._lib.spo_profile(self._h, 1 if enable else 0))
 

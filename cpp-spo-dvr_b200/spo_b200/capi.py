@@ -31,7 +31,7 @@ EXPORTS = [
     "spo_profile_count", "spo_profile_entry", "spo_device_bytes", "spo_last_launch_count",
     "spo_block_densities_noalloc", "spo_analysis_setup", "spo_bk_coefficients", "spo_s_matrix_sums",
     "spo_describe", "spo_averages", "spo_ensemble_create", "spo_ensemble_step", "spo_ensemble_launch_count",
-    "spo_ensemble_last_error", "spo_ensemble_destroy",
+    "spo_ensemble_last_error", "spo_ensemble_destroy", "spo_test_wait_timeout",
 ]
 NOALLOC_MAX_BLOCKS = 65536
 
@@ -107,6 +107,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.spo_profile_count.argtypes = [h, _ip]
     lib.spo_profile_entry.argtypes = [h, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp, _ip, _dp]
     lib.spo_device_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.spo_test_wait_timeout.argtypes = [h, ctypes.c_int, ctypes.c_int]
     lib.spo_analysis_setup.argtypes = [h, ctypes.POINTER(SpoAnalysisDesc)]
     lib.spo_bk_coefficients.argtypes = [h, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
     lib.spo_s_matrix_sums.argtypes = [h, _dp]

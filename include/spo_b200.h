@@ -214,6 +214,16 @@ int spo_profile_count(const spo_handle* h, int* n);
 int spo_profile_entry(const spo_handle* h, int i, char* name, int name_len, double* total_ms, int* launches,
                       double* bytes_per_launch);
 
+/* Failure-detection test of the bounded device-side waits (no counterpart in the reference, whose kernels
+ * do not wait on barriers). With unmatched_bytes > 0 (a multiple of 16, at most 4096) every item of the
+ * potential kernels that move their data by bulk asynchronous copies (potential5, potential6) announces that
+ * many bytes more on its first barrier than its copies deliver, so the barrier's phase cannot complete;
+ * every copy stays valid and lands. Each wait gives up after poll_limit polls (<= 0: the default limit), the
+ * block records the failure, waits (bounded) for its work in flight and leaves, and the next
+ * spo_propagate_analysis_step returns SPO_ERR_TIMEOUT; the wave packet is then undefined until the next
+ * spo_upload_state. spo_test_wait_timeout(h, 0, 0) restores normal operation. */
+int spo_test_wait_timeout(spo_handle* h, int poll_limit, int unmatched_bytes);
+
 /* Bytes of device memory the handle holds. */
 int spo_device_bytes(const spo_handle* h, unsigned long long* bytes);
 

@@ -56,7 +56,7 @@ def make(case, kernels, precision, tiles=None):
 
 @pytest.mark.parametrize("shape", list(SHAPES))
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("kernels", ["v2", "v3", "v4", "v5"])
+@pytest.mark.parametrize("kernels", ["v2", "v3", "v4", "v5", "v6"])
 def test_register_kernels_match_general_kernels(shape, precision, kernels):
     from spo_b200 import capi, workload
     case = workload.config_case(SHAPES[shape])
@@ -66,8 +66,10 @@ def test_register_kernels_match_general_kernels(shape, precision, kernels):
     tol_stage, tol_step = (1e-12, 1e-11) if precision == "fp64" else (2e-6, 2e-5)
     ref = make(case, "v1", precision)
     new = make(case, kernels, precision)
-    if kernels == "v5" and precision == "fp64":  # potential5 is the mixed form's
+    if kernels in ("v5", "v6") and precision == "fp64":  # potential5 and 6 are the mixed form's
         assert "potential=potential4" in new.describe(), new.describe()
+    elif kernels == "v6" and shape == "xy16":  # potential6 needs theta 16 x phi 32: the best one below it
+        assert "potential=potential5" in new.describe(), new.describe()
     else:
         assert f"potential=potential{kernels[1]}" in new.describe(), new.describe()
     for be in (ref, new):
@@ -310,3 +312,36 @@ def test_potential5_pads_theta_12_and_14(j_max):
         p, c = be.wave_packet_on_host()
         assert rel_l2(p, p_step) < 2e-5 and rel_l2(c, c_step) < 2e-5, kernels
         be.close()
+
+
+@pytest.mark.parametrize("nxy", [8, 16, 6])
+def test_potential6_agrees_with_potential5_and_the_general_kernel(nxy):
+    """potential6 (both theta contractions as split-precision TF32 tcgen05 GEMMs, 64-column tiles) on the
+    configuration-2 angular grid (theta 16 x phi 32, JMax = MJMax = 15, n_rot 256): one tile (8 x 8), four
+    tiles (16 x 16) and a partial tile (6 x 6: 36 columns). The potential stage alone against the general
+    kernel and potential5 to FP32 rounding (2e-6 of the largest value), then two analysis steps to 2e-5
+    relative L2."""
+    from spo_b200 import capi, workload
+    case = workload.config_case({"nz": 24, "nr": 16, "nx": nxy, "ny": nxy, "j_max": 15, "mj_max": 15,
+                                 "nz_specular": 64, "nz_potential": 14})
+    assert case.m["n_theta"] == 16 and case.m["n_phi"] == 32 and case.n_rot == 256
+    rng = np.random.default_rng(23)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    stage, step = {}, {}
+    for kernels in ("v1", "v5", "v6"):
+        be = make(case, kernels, "mixed")
+        if kernels != "v1":
+            assert f"potential=potential{kernels[1]}" in be.describe(), be.describe()
+        be.read_wave_packet(psi0, chi0)
+        be.apply_stage(capi.STAGE_POTENTIAL)
+        stage[kernels] = be.wave_packet_on_host()
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        be.propagate_analysis_step()
+        step[kernels] = be.wave_packet_on_host()
+        be.close()
+    for ref in ("v1", "v5"):
+        assert rel_err(stage["v6"][0], stage[ref][0]) < 2e-6, (ref, rel_err(stage["v6"][0], stage[ref][0]))
+        assert rel_err(stage["v6"][1], stage[ref][1]) < 2e-6, ref
+        assert rel_l2(step["v6"][0], step[ref][0]) < 2e-5 and rel_l2(step["v6"][1], step[ref][1]) < 2e-5, ref
