@@ -22,6 +22,7 @@
 #include <complex>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -180,7 +181,9 @@ template <typename T, int N1, int N2, int TB>
 bool launch_axis2_tb(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
   constexpr int NS = N1 > N2 ? N1 : N2;
   constexpr int N = N1 * N2;
-  const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(N) * TB + 2 * N);
+  // the tile, then the factors (mixed form: their parts, spo::fmul_t) and the twiddles (mixed form: and their low parts)
+  const std::size_t smem =
+      sizeof(spo::Vec<T>) * (static_cast<std::size_t>(N) * TB + (sizeof(T) == 4 ? spo::kFactorParts + 2 : 2) * N);
   static unsigned long long configured = 0;
   allow_smem(spo::axis2_kernel<T, N1, N2, TB>, smem, configured, "axis2 smem");
   if (a.persistent && a.window == 0) {
@@ -235,7 +238,7 @@ bool launch_axis2(int n, const spo::Axis2Args<T>& a, long long outer, cudaStream
     case 24: return launch_axis2_n<T, 4, 6>(a, outer, stream);
     case 32: return launch_axis2_n<T, 4, 8>(a, outer, stream);
     case 40: return launch_axis2_n<T, 5, 8>(a, outer, stream);
-    case 48: return launch_axis2_n<T, 6, 8>(a, outer, stream);
+    case 48: return launch_axis2_n<T, 3, 16>(a, outer, stream);  // the odd factor in the first level only
     case 56: return launch_axis2_n<T, 7, 8>(a, outer, stream);
     case 64: return launch_axis2_n<T, 8, 8>(a, outer, stream);
     case 80: return launch_axis2_n<T, 8, 10>(a, outer, stream);
@@ -272,7 +275,8 @@ inline bool xy2_supported(int n) { return n == 2 || n == 4 || n == 6 || n == 8 |
 template <typename T, int NX, int NY, int TB>
 void launch_xy2_tb(const spo::XyArgs<T>& a, long long n_zr, cudaStream_t stream) {
   constexpr int NS = NX > NY ? NX : NY;
-  const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(NX * NY) * TB + NX * NY);
+  const std::size_t smem =
+      sizeof(spo::Vec<T>) * (static_cast<std::size_t>(NX * NY) * TB + (sizeof(T) == 4 ? spo::kFactorParts : 1) * NX * NY);
   if (a.persistent) {
     static unsigned long long configured_p = 0;
     static int blocks_p = 0;
@@ -320,7 +324,7 @@ template <typename T>
 std::size_t pot2_smem(int cb, int n_rot, int nt, int nphi, long long n_xy) {
   return sizeof(spo::Vec<T>) * (static_cast<std::size_t>(cb) * n_rot + static_cast<std::size_t>(cb) * nt * (nphi + 1) +
                                 n_xy + 32) +
-         sizeof(T) * static_cast<std::size_t>(nt) * n_rot;
+         (sizeof(T) == 4 ? 2 : 1) * sizeof(T) * static_cast<std::size_t>(nt) * n_rot;  // matrix (+ low parts)
 }
 
 template <typename T, int NPHI, int CB>
@@ -513,6 +517,72 @@ class Profiler {
   std::vector<KernelRecord> records_;
   std::size_t used_ = 0;
 };
+
+// Rounds a matrix to FP32 row by row so that each row's sum of squares is as close to its FP64 value as
+// the roundings allow: every entry takes one of its two FP32 neighbours, chosen by a meet-in-the-middle
+// search over the entries' alternatives (rows of up to 24 non-zero entries; longer rows keep the nearest
+// rounding). A matrix applied with its transpose at every time step (the theta contractions) then changes
+// the norm of a state only by the unbiased rounding of the arithmetic, not by its entries' rounding.
+inline std::vector<float> norm_preserving_rows(const std::vector<double>& m, int rows, int stride) {
+  std::vector<float> out(m.size());
+  for (std::size_t i = 0; i < m.size(); ++i) out[i] = static_cast<float>(m[i]);
+  for (int r = 0; r < rows; ++r) {
+    const std::size_t base = static_cast<std::size_t>(r) * stride;
+    double target = 0.0, have = 0.0;
+    std::vector<int> idx;
+    std::vector<double> delta;  // change of the sum of squares when entry idx[k] takes its other neighbour
+    std::vector<float> other;
+    for (int c = 0; c < stride; ++c) {
+      const double v = m[base + c];
+      const float f = out[base + c];
+      target += v * v;
+      have += static_cast<double>(f) * f;
+      if (v == 0.0 || static_cast<double>(f) == v) continue;
+      const float g = static_cast<double>(f) < v ? std::nextafter(f, std::numeric_limits<float>::infinity())
+                                                 : std::nextafter(f, -std::numeric_limits<float>::infinity());
+      idx.push_back(c);
+      other.push_back(g);
+      delta.push_back(static_cast<double>(g) * g - static_cast<double>(f) * f);
+    }
+    const int n = static_cast<int>(idx.size());
+    if (n == 0 || n > 24) continue;
+    const double need = target - have;
+    const int na = n / 2, nb = n - na;
+    std::vector<std::pair<double, unsigned>> right;
+    for (unsigned mask = 0; mask < (1u << nb); ++mask) {
+      double sum = 0.0;
+      for (int k = 0; k < nb; ++k)
+        if (mask >> k & 1u) sum += delta[na + k];
+      right.emplace_back(sum, mask);
+    }
+    std::sort(right.begin(), right.end());
+    double best = std::fabs(need);
+    unsigned best_a = 0, best_b = 0;
+    for (unsigned mask = 0; mask < (1u << na); ++mask) {
+      double sum = 0.0;
+      for (int k = 0; k < na; ++k)
+        if (mask >> k & 1u) sum += delta[k];
+      const double want = need - sum;
+      auto it = std::lower_bound(right.begin(), right.end(), std::make_pair(want, 0u));
+      for (int step = 0; step < 2; ++step, --it) {
+        if (it != right.end()) {
+          const double err = std::fabs(want - it->first);
+          if (err < best) {
+            best = err;
+            best_a = mask;
+            best_b = it->second;
+          }
+        }
+        if (it == right.begin()) break;
+      }
+    }
+    for (int k = 0; k < na; ++k)
+      if (best_a >> k & 1u) out[base + idx[k]] = other[k];
+    for (int k = 0; k < nb; ++k)
+      if (best_b >> k & 1u) out[base + idx[na + k]] = other[na + k];
+  }
+  return out;
+}
 
 class StepBase {
  public:
@@ -1141,7 +1211,7 @@ class Step final : public StepBase {
     a.dir = dir;
     a.post = post;
     a.tb = axis_tile(plan.n, inner);
-    const std::size_t smem = sizeof(V) * (2 * static_cast<std::size_t>(plan.n) * a.tb + plan.n);
+    const std::size_t smem = sizeof(V) * (2 * static_cast<std::size_t>(plan.n) * a.tb + (sizeof(T) == 4 ? 2 : 1) * plan.n);
     const dim3 grid(static_cast<unsigned>((inner + a.tb - 1) / a.tb), static_cast<unsigned>(outer));
     prof_.begin(stream_);
     spo::axis_pass_kernel<T><<<grid, 256, smem, stream_>>>(a);
@@ -1164,15 +1234,64 @@ class Step final : public StepBase {
     return static_cast<U*>(arena_.alloc(sizeof(U) * n));
   }
 
+  // A complex table on the device. The mixed form stores each value rounded to FP32 followed by the n
+  // roundings of the remainders (value - rounded value): kernels apply the pair as one constant exact to
+  // ~2^-48 (spo::cmul2), so that a table applied at every time step does not change the norm
+  // systematically through its own rounding.
   V* upload_complex(const std::vector<cplx>& v) {
-    std::vector<V> h(v.size());
-    for (std::size_t i = 0; i < v.size(); ++i) {
+    const std::size_t n = v.size();
+    std::vector<V> h((sizeof(T) == 4 ? 2 : 1) * n);
+    for (std::size_t i = 0; i < n; ++i) {
       h[i].x = static_cast<T>(v[i].real());
       h[i].y = static_cast<T>(v[i].imag());
+      if constexpr (sizeof(T) == 4) {
+        h[n + i].x = static_cast<T>(v[i].real() - static_cast<double>(h[i].x));
+        h[n + i].y = static_cast<T>(v[i].imag() - static_cast<double>(h[i].y));
+      }
     }
-    V* d = dev<V>(v.size());
+    V* d = dev<V>(h.size());
     check_cuda(cudaMemcpy(d, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice), "upload table");
     return d;
+  }
+  // A real matrix with, in the mixed form, its low parts: the entries v (as T) followed by the roundings of
+  // exact - v; the FP64 form uploads exact.
+  // A table of factors s e^{i phi} (s >= 0 real: kinetic and rotation phases with FFT scales or absorbers). The
+  // mixed form stores g = e^{i phi} - 1 (n values), the roundings of g's remainders (n values) and, per factor,
+  // (s, the rounding of s's remainder) (n pairs): spo::fmul_t applies the factor as s (x + x g), which FP32 rounds
+  // without the bias of a near-unity phase product. The FP64 form stores the factors.
+  V* upload_factor(const std::vector<cplx>& f) {
+    if constexpr (sizeof(T) == 4) {
+      const std::size_t n = f.size();
+      std::vector<V> h(spo::kFactorParts * n);
+      for (std::size_t i = 0; i < n; ++i) {
+        const double sc = std::abs(f[i]);
+        const cplx g = sc > 0.0 ? cplx(f[i].real() / sc - 1.0, f[i].imag() / sc) : cplx(-1.0, 0.0);
+        h[i].x = static_cast<T>(g.real());
+        h[i].y = static_cast<T>(g.imag());
+        h[n + i].x = static_cast<T>(g.real() - static_cast<double>(h[i].x));
+        h[n + i].y = static_cast<T>(g.imag() - static_cast<double>(h[i].y));
+        h[2 * n + i].x = static_cast<T>(sc);
+        h[2 * n + i].y = static_cast<T>(sc - static_cast<double>(h[2 * n + i].x));
+      }
+      V* d = dev<V>(h.size());
+      check_cuda(cudaMemcpy(d, h.data(), sizeof(V) * h.size(), cudaMemcpyHostToDevice), "upload table");
+      return d;
+    } else {
+      return upload_complex(f);
+    }
+  }
+  T* upload_real_lo(const std::vector<double>& v, const std::vector<double>& exact) {
+    if constexpr (sizeof(T) == 4) {
+      std::vector<double> both(2 * v.size());
+      for (std::size_t i = 0; i < v.size(); ++i) {
+        const double hi = static_cast<float>(v[i]);
+        both[i] = hi;
+        both[v.size() + i] = exact[i] - hi;
+      }
+      return upload_real(both);
+    } else {
+      return upload_real(exact);
+    }
   }
   T* upload_real(const std::vector<double>& v) {
     std::vector<T> h(v.begin(), v.end());
@@ -1218,19 +1337,19 @@ class Step final : public StepBase {
       for (auto& x : v) x *= f;
       return v;
     };
-    zk_full_ = upload_complex(scaled(complex_array(d.z_kinetic_full, s.nz, "z_kinetic_full"), 1.0 / s.nz));
-    zk_half_ = upload_complex(scaled(complex_array(d.z_kinetic_half, s.nz, "z_kinetic_half"), 1.0 / s.nz));
-    rk_full_ = upload_complex(scaled(complex_array(d.r_kinetic_full, s.nr, "r_kinetic_full"), 1.0 / s.nr));
-    rk_half_ = upload_complex(scaled(complex_array(d.r_kinetic_half, s.nr, "r_kinetic_half"), 1.0 / s.nr));
+    zk_full_ = upload_factor(scaled(complex_array(d.z_kinetic_full, s.nz, "z_kinetic_full"), 1.0 / s.nz));
+    zk_half_ = upload_factor(scaled(complex_array(d.z_kinetic_half, s.nz, "z_kinetic_half"), 1.0 / s.nz));
+    rk_full_ = upload_factor(scaled(complex_array(d.r_kinetic_full, s.nr, "r_kinetic_full"), 1.0 / s.nr));
+    rk_half_ = upload_factor(scaled(complex_array(d.r_kinetic_half, s.nr, "r_kinetic_half"), 1.0 / s.nr));
     const double sx = s.nx > 1 ? d.fft_scale_x : 1.0;
     const double sy = s.ny > 1 ? d.fft_scale_y : 1.0;
     const double xy_scale = (sx * sy) * ((1.0 / (s.nx * sx)) * (1.0 / (s.ny * sy)));
-    xyk_full_ = upload_complex(scaled(complex_array(d.xy_kinetic_full, nxy, "xy_kinetic_full"), xy_scale));
-    xyk_half_ = upload_complex(scaled(complex_array(d.xy_kinetic_half, nxy, "xy_kinetic_half"), xy_scale));
+    xyk_full_ = upload_factor(scaled(complex_array(d.xy_kinetic_full, nxy, "xy_kinetic_full"), xy_scale));
+    xyk_half_ = upload_factor(scaled(complex_array(d.xy_kinetic_half, nxy, "xy_kinetic_half"), xy_scale));
     const double sz = d.fft_scale_z, sr = d.fft_scale_r;
     const double spec_scale = (sz * sr) * ((1.0 / (s.nzs * sz)) * (1.0 / (s.nr * sr)));
-    spec_full_ = upload_complex(scaled(complex_array(d.specular_kinetic_full, s.n_chi(), "specular_kinetic_full"), spec_scale));
-    spec_half_ = upload_complex(scaled(complex_array(d.specular_kinetic_half, s.n_chi(), "specular_kinetic_half"), spec_scale));
+    spec_full_ = upload_factor(scaled(complex_array(d.specular_kinetic_full, s.n_chi(), "specular_kinetic_full"), spec_scale));
+    spec_half_ = upload_factor(scaled(complex_array(d.specular_kinetic_half, s.n_chi(), "specular_kinetic_half"), spec_scale));
 
     // Potential-step factors (src/propagation/potential_operator.cpp:15-26) and the specular grid's
     // W factors (src/propagation/specular_operator.cpp:11-19, 58-71), merged in FP64.
@@ -1256,24 +1375,24 @@ class Step final : public StepBase {
         if (s.nr != 1 && ir >= s.ra && ir <= s.rb) f *= opt_r[ir];
         spec_w[ir + static_cast<std::size_t>(s.nr) * iz] = f;
       }
-    rot_half_ = upload_complex([&] {
+    rot_half_ = upload_factor([&] {
       std::vector<cplx> v(rot.size());
       for (int ir = 0; ir < s.nr; ++ir)
         for (int irot = 0; irot < s.n_rot; ++irot)
           v[static_cast<std::size_t>(ir) * s.n_rot + irot] = rot[irot + static_cast<std::size_t>(s.n_rot) * ir];
       return v;
     }());
-    before_ = upload_complex(before);
-    gas_step_ = upload_complex(gas_step);
-    spec_w_ = upload_complex(spec_w);
+    before_ = upload_factor(before);
+    gas_step_ = upload_factor(gas_step);
+    spec_w_ = upload_factor(spec_w);
     opt_z_ = upload_real(opt_z);
 
     const std::vector<cplx> shf = complex_array(d.shift_forward, nxy, "shift_forward");
     shift_host_ = shf;
     const bool shift = std::any_of(shf.begin(), shf.end(), [](const cplx& c) { return c.real() != 1.0 || c.imag() != 0.0; });
     if (shift) {
-      shift_f_ = upload_complex(shf);
-      shift_b_ = upload_complex(complex_array(d.shift_backward, nxy, "shift_backward"));
+      shift_f_ = upload_factor(shf);
+      shift_b_ = upload_factor(complex_array(d.shift_backward, nxy, "shift_backward"));
     }
     const V* sp2sc = upload_complex(complex_array(d.specular_to_scattering, nxy, "specular_to_scattering"));
     const V* sc2sp = upload_complex(complex_array(d.scattering_to_specular, nxy, "scattering_to_specular"));
@@ -1296,7 +1415,23 @@ class Step final : public StepBase {
       }
     }
     require(total_j == s.n_rot, "mj blocks do not cover the rotational basis");
-    const std::vector<double> legendre = real_array(d.legendre, static_cast<std::size_t>(off), "legendre");
+    std::vector<double> legendre = real_array(d.legendre, static_cast<std::size_t>(off), "legendre");
+    const std::vector<double> legendre64 = legendre;  // the FP64 matrix (the low parts of the mixed form's tables)
+    if constexpr (sizeof(T) == 4) {
+      // The mixed form's matrix, rounded once for every potential kernel so that each rotational state's
+      // sum of squares over theta keeps its FP64 value: the forward and the transposed contraction of a step
+      // multiply the state by that sum (times nphi), every step (norm_preserving_rows).
+      std::vector<double> by_state(static_cast<std::size_t>(s.n_rot) * s.nt);
+      for (int b = 0; b < s.n_blocks; ++b)
+        for (int t = 0; t < s.nt; ++t)
+          for (int j = 0; j < size[b]; ++j)
+            by_state[static_cast<std::size_t>(first[b] + j) * s.nt + t] = legendre[offset[b] + t * size[b] + j];
+      const std::vector<float> rounded = norm_preserving_rows(by_state, s.n_rot, s.nt);
+      for (int b = 0; b < s.n_blocks; ++b)
+        for (int t = 0; t < s.nt; ++t)
+          for (int j = 0; j < size[b]; ++j)
+            legendre[offset[b] + t * size[b] + j] = rounded[static_cast<std::size_t>(first[b] + j) * s.nt + t];
+    }
 
     // Symmetry maps, expanded to one phi map per (x, y) point.
     const std::vector<int> rep = int_array(d.representative_of, nxy, "representative_of");
@@ -1326,14 +1461,16 @@ class Step final : public StepBase {
     // exp(i A) on the device in FP64, chunk by chunk through the staging buffer.
     const long long n_e = s.n_expia();
     require(d.potential != nullptr || n_e == 0, "potential is null");
-    expia_ = dev<V>(std::max<long long>(n_e, 1));
+    // The mixed form keeps, after the n_e table entries, their n_e modulus corrections (FP16, spo::exp_mul).
+    expia_ = dev<V>(std::max<long long>(n_e + (sizeof(T) == 4 ? (n_e + 3) / 4 : 0), 1));
+    __half* exp_mod = sizeof(T) == 4 ? reinterpret_cast<__half*>(expia_ + n_e) : nullptr;
     double* vstage = reinterpret_cast<double*>(staging_);
     const long long chunk = 2 * staging_elems_;
     for (long long i = 0; i < n_e; i += chunk) {
       const long long m = std::min(chunk, n_e - i);
       check_cuda(cudaMemcpyAsync(vstage, d.potential + i, sizeof(double) * m, cudaMemcpyHostToDevice, stream_),
                  "upload potential");
-      spo::exp_potential_kernel<T><<<1184, 256, 0, stream_>>>(vstage, expia_ + i, m, s.dt);
+      spo::exp_potential_kernel<T><<<1184, 256, 0, stream_>>>(vstage, expia_ + i, exp_mod ? exp_mod + i : nullptr, m, s.dt);
       check_cuda(cudaGetLastError(), "exp_potential launch");
       check_cuda(cudaStreamSynchronize(stream_), "exp_potential");
     }
@@ -1348,15 +1485,15 @@ class Step final : public StepBase {
                                                      "FFT length too long for shared memory");
     xy_tb_ = 1;
     while (xy_tb_ < 32 && xy_tb_ < s.n_rot && 2ull * nxy * (2 * xy_tb_) * sizeof(V) <= (96u << 10)) xy_tb_ *= 2;
-    xy_smem_ = sizeof(V) * (2 * nxy * xy_tb_ + s.nx + s.ny);
+    xy_smem_ = sizeof(V) * (2 * nxy * xy_tb_ + (sizeof(T) == 4 ? 2 : 1) * (s.nx + s.ny));
     require(xy_smem_ <= static_cast<std::size_t>(smem_optin), "nx*ny too large for the xy pass");
     check_cuda(cudaFuncSetAttribute(spo::xy_pass_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin),
                "xy smem");
 
     const int ld = s.nphi + 1;
     auto pot_bytes = [&](int cb) {
-      return sizeof(V) * (static_cast<std::size_t>(cb) * s.n_rot + 2ull * cb * s.nt * ld + s.nphi + nxy + 32) +
-             sizeof(T) * static_cast<std::size_t>(s.nt) * s.n_rot;
+      return sizeof(V) * (static_cast<std::size_t>(cb) * s.n_rot + 2ull * cb * s.nt * ld + (sizeof(T) == 4 ? 2 : 1) * s.nphi + nxy + 32) +
+             (sizeof(T) == 4 ? 2 : 1) * sizeof(T) * static_cast<std::size_t>(s.nt) * s.n_rot;
     };
     int cb = 1;
     while (cb < 16 && cb < nxy && pot_bytes(cb + 1) <= std::min<std::size_t>(smem_optin, 112u << 10)) ++cb;
@@ -1379,7 +1516,7 @@ class Step final : public StepBase {
     pot_.cb = cb;
     pot_.pphi = plan_phi_;
     pot_.twphi = tw_phi_;
-    pot_.legendre = upload_real(legendre);
+    pot_.legendre = upload_real_lo(legendre, legendre64);
     pot_.block_first = upload_int(first);
     pot_.block_size = upload_int(size);
     pot_.block_slot = upload_int(slot);
@@ -1391,6 +1528,7 @@ class Step final : public StepBase {
     pot_.sp2sc = sp2sc;
     pot_.sc2sp = sc2sp;
     pot_.expia = expia_;
+    pot_.exp_mod = exp_mod;
     pot_.rep_of = upload_int(rep);
     pot_.phi_map = upload_int(phi_map);
 
@@ -1409,13 +1547,15 @@ class Step final : public StepBase {
       }
     }
     if (pot2_cb_ > 0) {
-      std::vector<double> leg_t(legendre.size());
+      std::vector<double> leg_t(legendre.size()), leg_t64(legendre.size());
       for (int b = 0; b < s.n_blocks; ++b)
         for (int t = 0; t < s.nt; ++t)
-          for (int j = 0; j < size[b]; ++j)
+          for (int j = 0; j < size[b]; ++j) {
             leg_t[offset[b] + j * s.nt + t] = legendre[offset[b] + t * size[b] + j];
+            leg_t64[offset[b] + j * s.nt + t] = legendre64[offset[b] + t * size[b] + j];
+          }
       pot2_.p = pot_;
-      pot2_.legendre_t = upload_real(leg_t);
+      pot2_.legendre_t = upload_real_lo(leg_t, leg_t64);
       pot2_.cb = pot2_cb_;
       bool identity = s.n_rep == nxy;
       for (long long ixy = 0; ixy < nxy && identity; ++ixy) {
@@ -1439,11 +1579,14 @@ class Step final : public StepBase {
       const int cb = s.nt <= 4 ? 16 : 8;  // FP64 at cb = 32 spills; 16 columns keep 4+ warps per block
       const std::size_t need = pot3_smem<T>(cb, jp, s.nt, s.nphi);
       if (need <= static_cast<std::size_t>(smem_optin)) {
-        std::vector<double> leg_slot(static_cast<std::size_t>(s.nphi) * jp * s.nt, 0.0);
+        std::vector<double> leg_slot(static_cast<std::size_t>(s.nphi) * jp * s.nt, 0.0), leg_slot64(leg_slot);
         for (int b = 0; b < s.n_blocks; ++b)
           for (int j = 0; j < size[b]; ++j)
-            for (int t = 0; t < s.nt; ++t)
-              leg_slot[(static_cast<std::size_t>(slot[b]) * jp + j) * s.nt + t] = legendre[offset[b] + t * size[b] + j];
+            for (int t = 0; t < s.nt; ++t) {
+              const std::size_t k = (static_cast<std::size_t>(slot[b]) * jp + j) * s.nt + t;
+              leg_slot[k] = legendre[offset[b] + t * size[b] + j];
+              leg_slot64[k] = legendre64[offset[b] + t * size[b] + j];
+            }
         pot3_cb_ = cb;
         pot3_smem_ = need;
         pot3_chunks_ = static_cast<int>((nxy + cb - 1) / cb);
@@ -1451,7 +1594,7 @@ class Step final : public StepBase {
         pot3_args_.cb = cb;
         pot3_args_.slot_first = upload_int(slot_first);
         pot3_args_.slot_nj = upload_int(slot_nj);
-        pot3_args_.legendre_slot = upload_real(leg_slot);
+        pot3_args_.legendre_slot = upload_real_lo(leg_slot, leg_slot64);
         pot3_args_.jp = jp;
       }
     }
@@ -1635,7 +1778,6 @@ class Step final : public StepBase {
     if (use_v2_ && pot3_cb_ > 0) pot_kind_ = 3;
     if (use_v2_ && pot4_kernel_) pot_kind_ = 4;
     if (use_v2_ && pot5_kernel_) pot_kind_ = 5;
-    if (use_v2_ && pot6_kernel_) pot_kind_ = 6;
     pot_source_ = "default";
     if (const char* env = std::getenv("SPO_B200_KERNELS")) {
       const std::string k(env);

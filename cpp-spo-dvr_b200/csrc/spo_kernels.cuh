@@ -7,9 +7,11 @@
 // global loads and stores of every kernel are coalesced, whatever axis is transformed.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 namespace spo {
 
@@ -36,6 +38,99 @@ template <typename V> SPO_HD V cmul(V a, V b) {
 }
 template <typename V> SPO_HD V cconj(V a) { return cmake<V>(a.x, -a.y); }
 template <typename V> SPO_HD V cscale(V a, decltype(V::x) s) { return cmake<V>(a.x * s, a.y * s); }
+// a * (w + wl) for a constant held as two values: w (its rounding) and wl (the rounding of the rest).
+// The mixed form keeps every constant factor (FFT twiddles, kinetic, rotation and coupling factors) this
+// way: an FP32 constant of modulus 1 is off by up to 2^-24 in modulus, and the same constant applied at
+// every time step to the same components changes the norm systematically (~1e-7 per step); held as
+// w + wl it is exact to ~2^-48, and only the unbiased rounding of the product remains. The small terms are
+// summed first, then the large ones, each by a fused multiply-add.
+SPO_HD float2 cmul2(float2 a, float2 w, float2 wl) {
+  const float cr = fmaf(a.x, wl.x, -a.y * wl.y);
+  const float ci = fmaf(a.x, wl.y, a.y * wl.x);
+  return make_float2(fmaf(a.x, w.x, fmaf(-a.y, w.y, cr)), fmaf(a.x, w.y, fmaf(a.y, w.x, ci)));
+}
+// The FP64 form keeps its constants in one double each (wl is ignored).
+SPO_HD double2 cmul2(double2 a, double2 w, double2) {
+  return make_double2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+// a * (w + wl) as one FP64 product rounded once (mixed form). Twiddles of transform lengths with an odd
+// factor (48 = 3 x 16, ...) need it: with FP32 partial sums their products still drift the norm of a pass
+// by ~1e-9, the same sign every pass; powers of two do not (cmul2 suffices).
+SPO_HD float2 cmul_dd(float2 a, float2 w, float2 wl) {
+  const double wx = static_cast<double>(w.x) + wl.x, wy = static_cast<double>(w.y) + wl.y;
+  const double ax = a.x, ay = a.y;
+  return make_float2(static_cast<float>(ax * wx - ay * wy), static_cast<float>(ax * wy + ay * wx));
+}
+SPO_HD double2 cmul_dd(double2 a, double2 w, double2) {
+  return make_double2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+
+// The low part of a table entry: complex tables of the mixed form hold n values followed by their n low
+// parts (see cmul2); the FP64 form's tables hold the n values only and have no low part.
+template <typename V>
+__device__ __forceinline__ V lo_part(const V* table, long long n, long long k) {
+  if constexpr (sizeof(V) == 8) return table[n + k];
+  else return V{0.0, 0.0};
+}
+// a * table[k] with the table's low part (mixed form).
+template <typename V>
+__device__ __forceinline__ V cmul_t(V a, const V* table, long long n, long long k) {
+  return cmul2(a, table[k], lo_part(table, n, k));
+}
+
+// The low part of a real matrix entry k of a table of n entries: the mixed form's Legendre tables of the
+// small-grid potential kernels hold their n entries followed by the n roundings of the remainders
+// (FP64 value - entry), so that a contraction and its transpose keep the norm of a state to ~2^-48 whatever
+// the number of theta points; FP64 tables have no low part.
+template <typename T>
+__device__ __forceinline__ T lo_real(const T* table, long long n, long long k) {
+  if constexpr (sizeof(T) == 4) return table[n + k];
+  else return T(0);
+}
+// s + w f for a real matrix entry held as w + wl (mixed form; the small term first).
+template <typename V>
+__device__ __forceinline__ V cadd_scaled(V s, V f, decltype(V::x) w, decltype(V::x) wl) {
+  if constexpr (sizeof(V) == 8) return cmake<V>(fmaf(w, f.x, fmaf(wl, f.x, s.x)), fmaf(w, f.y, fmaf(wl, f.y, s.y)));
+  else return cmake<V>(s.x + w * f.x, s.y + w * f.y);
+}
+
+// x * exp(i A) from the exp(i A) table. The mixed form holds g = exp(i A) - 1 (FP32; applied as x + x g, see
+// fmul_t) and, per entry, m = 1/|1 + g| - 1 (FP16, a multiple of 2^-24): x (1 + g)(1 + m) = x + x (g + m (1 + g)).
+// Without m a point's norm would change by |1 + g|^2 - 1 (~1e-8) every step, for all points of equal V the same
+// way. The FP64 form holds exp(i A) itself.
+template <typename V>
+__device__ __forceinline__ V exp_mul(V x, V e, const __half* mod, long long idx) {
+  if constexpr (sizeof(V) == 8) {
+    const float m = __half2float(__ldg(mod + idx)) * 5.9604644775390625e-8f;  // 2^-24
+    return cadd(x, cmul2(x, e, make_float2(m * (1.0f + e.x), m * e.y)));
+  } else {
+    return cmul(e, x);
+  }
+}
+
+// x times entry k of a factor table: a factor s e^{i phi} with s >= 0 real (a kinetic or rotation phase, with an
+// FFT scale or an absorber). The mixed form holds each factor as g = e^{i phi} - 1 (n values), the low parts of g
+// (n values) and (s, the low part of s) (n pairs), and forms s (x + x g): a near-unity phase applied as x e^{i phi}
+// in FP32 rounds its result with a bias (~4e-10 of the norm per product for the small phases of the low kinetic
+// momenta), x + x g does not (the correction x g is small and carries its own precision). The FP64 form's tables
+// hold the factors themselves.
+template <typename V>
+__device__ __forceinline__ V fmul_parts(V x, V g, V gl, V sc) {
+  if constexpr (sizeof(V) == 8) {
+    const float2 z = cadd(x, cmul2(x, g, gl));
+    return make_float2(fmaf(z.x, sc.x, z.x * sc.y), fmaf(z.y, sc.x, z.y * sc.y));
+  } else {
+    return cmul(g, x);
+  }
+}
+template <typename V>
+__device__ __forceinline__ V fmul_t(V x, const V* table, long long n, long long k) {
+  if constexpr (sizeof(V) == 8) return fmul_parts(x, table[k], table[n + k], table[2 * n + k]);
+  else return cmul(table[k], x);
+}
+// Entries of a mixed-form factor table per value: g, its low part, the scale pair.
+constexpr int kFactorParts = 3;
+
 // i * s * a for s = +1 or -1.
 template <typename V> SPO_HD V cimul(V a, int s) {
   return s > 0 ? cmake<V>(-a.y, a.x) : cmake<V>(a.y, -a.x);
@@ -52,10 +147,16 @@ struct FftPlan {
   int radix[kMaxStages];
 };
 
-// w^q for the r-th roots of unity, read from the length-n table tw[k] = exp(-2 pi i k / n).
+// w^q for the r-th roots of unity, read from the length-n table tw[k] = exp(-2 pi i k / n), and its low
+// part (mixed form: the n low parts follow the table in shared memory).
 template <typename V>
 __device__ __forceinline__ V root_of(const V* tw, int n, int r, int q, int sign) {
   V w = tw[(q % r) * (n / r)];
+  return sign > 0 ? cconj(w) : w;
+}
+template <typename V>
+__device__ __forceinline__ V root_lo_of(const V* tw, int n, int r, int q, int sign) {
+  V w = lo_part(tw, n, (q % r) * (n / r));
   return sign > 0 ? cconj(w) : w;
 }
 
@@ -88,20 +189,25 @@ __device__ __forceinline__ void small_dft(V (&v)[R], const V* tw, int n, int sig
     for (int t = 1; t <= H; ++t) out0 = cadd(out0, s[t]);
     V res[R];
     res[0] = out0;
+    // Each output pair summed in the accumulation type A (FP64 in the mixed form, see the register DFTs'
+    // odd primes) from the sums and differences, rounded once.
+    using Rl = decltype(V::x);
+    using A = std::conditional_t<sizeof(Rl) == 4, double, Rl>;
 #pragma unroll
     for (int q = 1; q <= H; ++q) {
-      V re = v[0];
-      decltype(V::x) im_re = 0, im_im = 0;
+      A rex = v[0].x, rey = v[0].y, im_re = 0, im_im = 0;
 #pragma unroll
       for (int t = 1; t <= H; ++t) {
         const V w = root_of(tw, n, R, t * q, sign);
-        re = cadd(re, cscale(s[t], w.x));
-        im_re += w.y * d[t].x;
-        im_im += w.y * d[t].y;
+        const V wl = root_lo_of(tw, n, R, t * q, sign);  // zero in the FP64 form
+        const A wx = static_cast<A>(w.x) + static_cast<A>(wl.x), wy = static_cast<A>(w.y) + static_cast<A>(wl.y);
+        rex += wx * static_cast<A>(s[t].x);
+        rey += wx * static_cast<A>(s[t].y);
+        im_re += wy * static_cast<A>(d[t].x);
+        im_im += wy * static_cast<A>(d[t].y);
       }
-      const V rot = cmake<V>(-im_im, im_re);  // i * sum Im(w) d
-      res[q] = cadd(re, rot);
-      res[R - q] = csub(re, rot);
+      res[q] = cmake<V>(static_cast<Rl>(rex - im_im), static_cast<Rl>(rey + im_re));  // re + i * sum Im(w) d
+      res[R - q] = cmake<V>(static_cast<Rl>(rex + im_im), static_cast<Rl>(rey - im_re));
     }
 #pragma unroll
     for (int t = 0; t < R; ++t) v[t] = res[t];
@@ -129,8 +235,12 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
 #pragma unroll
     for (int t = 1; t < R; ++t) {
       V w = tw[t * k * twstep];
-      if (sign > 0) w = cconj(w);
-      v[t] = cmul(v[t], w);
+      V wl = lo_part(tw, n, t * k * twstep);
+      if (sign > 0) {
+        w = cconj(w);
+        wl = cconj(wl);
+      }
+      v[t] = (n & (n - 1)) != 0 ? cmul_dd(v[t], w, wl) : cmul2(v[t], w, wl);  // see cmul_dd
     }
     small_dft<V, R>(v, tw, n, sign);
     const int o = (j / ns) * span + k;
@@ -195,11 +305,11 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a) {
   const int n = a.plan.n;
   const int tb = a.tb;
   V* buf1 = buf0 + n * tb;
-  V* tw = buf1 + n * tb;
+  V* tw = buf1 + n * tb;  // n values, then (mixed form) their n low parts
   const long long outer = blockIdx.y;
   const long long i0 = static_cast<long long>(blockIdx.x) * tb;
   const long long base = outer * n * a.inner + i0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) tw[k] = a.tw[k];
+  for (int k = threadIdx.x; k < (sizeof(T) == 4 ? 2 : 1) * n; k += blockDim.x) tw[k] = a.tw[k];
   for (int e = threadIdx.x; e < n * tb; e += blockDim.x) {
     const int k = e / tb, b = e % tb;
     V v = cmake<V>(0, 0);
@@ -216,8 +326,8 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a) {
   if (a.factor_mode != kNoFactor) {
     for (int e = threadIdx.x; e < n * tb; e += blockDim.x) {
       const int k = e / tb, b = e % tb;
-      const V f = a.factor_mode == kFactorAxis ? a.factor[k] : a.factor[(i0 + b) + a.inner * k];
-      cur[e] = cmul(f, cur[e]);
+      cur[e] = a.factor_mode == kFactorAxis ? fmul_t(cur[e], a.factor, n, k)
+                                            : fmul_t(cur[e], a.factor, a.inner * n, (i0 + b) + a.inner * k);
     }
     __syncthreads();
   }
@@ -229,7 +339,7 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a) {
     if (i0 + b < a.inner) {
       const long long g = base + k * a.inner + b;
       V v = cur[e];
-      if (a.post) v = cmul(a.post[g], v);
+      if (a.post) v = fmul_t(v, a.post, static_cast<long long>(gridDim.y) * n * a.inner, g);
       a.data[g] = v;
     }
   }
@@ -272,19 +382,20 @@ __global__ void __launch_bounds__(256) xy_pass_kernel(XyArgs<T> a) {
   const int tb = a.tb;
   V* buf0 = reinterpret_cast<V*>(smem_raw);
   V* buf1 = buf0 + nxy * tb;
+  constexpr int kParts = sizeof(T) == 4 ? 2 : 1;  // the mixed form's tables carry their low parts
   V* twx = buf1 + nxy * tb;
-  V* twy = twx + a.nx;
+  V* twy = twx + kParts * a.nx;
   const long long izr = blockIdx.y;
   const int r0 = blockIdx.x * tb;
-  for (int k = threadIdx.x; k < a.nx; k += blockDim.x) twx[k] = a.twx[k];
-  for (int k = threadIdx.x; k < a.ny; k += blockDim.x) twy[k] = a.twy[k];
+  for (int k = threadIdx.x; k < kParts * a.nx; k += blockDim.x) twx[k] = a.twx[k];
+  for (int k = threadIdx.x; k < kParts * a.ny; k += blockDim.x) twy[k] = a.twy[k];
   const long long col0 = izr * nxy;
   for (int e = threadIdx.x; e < nxy * tb; e += blockDim.x) {
     const int ixy = e / tb, b = e % tb;
     V v = cmake<V>(0, 0);
     if (r0 + b < a.n_rot) {
       v = a.psi[(col0 + ixy) * a.n_rot + r0 + b];
-      if (a.shift_f) v = cmul(v, a.shift_f[ixy]);
+      if (a.shift_f) v = fmul_t(v, a.shift_f, nxy, ixy);
     }
     buf0[e] = v;
   }
@@ -294,7 +405,7 @@ __global__ void __launch_bounds__(256) xy_pass_kernel(XyArgs<T> a) {
   V* oth = cur == buf0 ? buf1 : buf0;
   cur = smem_fft(cur, oth, twx, a.px, -1, a.ny * tb, a.ny * tb, 0, a.ny * tb);
   oth = cur == buf0 ? buf1 : buf0;
-  for (int e = threadIdx.x; e < nxy * tb; e += blockDim.x) cur[e] = cmul(a.factor[e / tb], cur[e]);
+  for (int e = threadIdx.x; e < nxy * tb; e += blockDim.x) cur[e] = fmul_t(cur[e], a.factor, nxy, e / tb);
   __syncthreads();
   cur = smem_fft(cur, oth, twx, a.px, +1, a.ny * tb, a.ny * tb, 0, a.ny * tb);
   oth = cur == buf0 ? buf1 : buf0;
@@ -306,9 +417,9 @@ __global__ void __launch_bounds__(256) xy_pass_kernel(XyArgs<T> a) {
     const int ixy = e / tb, b = e % tb;
     if (r0 + b < a.n_rot) {
       V v = cur[e];
-      if (a.shift_b) v = cmul(v, a.shift_b[ixy]);
+      if (a.shift_b) v = fmul_t(v, a.shift_b, nxy, ixy);
       if (gas) {
-        v = cmul(a.gas_step[ir * a.n_rot + r0 + b], v);
+        v = fmul_t(v, a.gas_step, static_cast<long long>(a.nr) * a.n_rot, ir * a.n_rot + r0 + b);
         v = cscale(v, oz);
       }
       a.psi[(col0 + ixy) * a.n_rot + r0 + b] = v;
@@ -344,6 +455,7 @@ struct PotArgs {
   const Vec<T>* sp2sc;        // n_xy
   const Vec<T>* sc2sp;        // n_xy
   const Vec<T>* expia;        // (izr, irep, theta, phi)
+  const __half* exp_mod;      // mixed form: per expia entry, (1/|entry| - 1) * 2^24 (see exp_mul); FP64: null
   const int* rep_of;          // n_xy
   const int* phi_map;         // n_xy * n_phi: phi_index of the operation of each ixy
 };
@@ -357,19 +469,21 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
   V* fbr = reinterpret_cast<V*>(smem_raw);   // cb * n_rot
   V* dvr0 = fbr + cb * n_rot;                // cb * nt * ld
   V* dvr1 = dvr0 + cb * dvr_col;             // cb * nt * ld
-  V* twp = dvr1 + cb * dvr_col;              // nphi
-  V* i0buf = twp + nphi;                     // n_xy
+  constexpr int kParts = sizeof(T) == 4 ? 2 : 1;  // the mixed form's twiddles carry their low parts
+  V* twp = dvr1 + cb * dvr_col;              // nphi (then nphi low parts)
+  V* i0buf = twp + kParts * nphi;            // n_xy
   V* red = i0buf + a.n_xy;                   // 32
-  T* leg = reinterpret_cast<T*>(red + 32);   // nt * n_rot
+  T* leg = reinterpret_cast<T*>(red + 32);   // nt * n_rot (then, mixed form, their low parts)
+  const long long n_leg = static_cast<long long>(nt) * n_rot;
   const int izr = blockIdx.x;
   const int ir = izr % a.nr;
   const int iz = izr / a.nr;
   const int i0 = a.initial_channel;
-  for (int k = threadIdx.x; k < nphi; k += blockDim.x) twp[k] = a.twphi[k];
-  for (int k = threadIdx.x; k < nt * n_rot; k += blockDim.x) leg[k] = a.legendre[k];
+  for (int k = threadIdx.x; k < kParts * nphi; k += blockDim.x) twp[k] = a.twphi[k];
+  for (int k = threadIdx.x; k < (sizeof(T) == 4 ? 2 : 1) * nt * n_rot; k += blockDim.x) leg[k] = a.legendre[k];
   const T oz = a.opt_z[iz];
   const V incoming = a.chi[ir + a.nr * iz];
-  const V rot_i0 = a.rot_half[ir * n_rot + i0];
+  const long long n_scale = static_cast<long long>(a.nr) * n_rot;  // entries of the scaling tables
   const long long col_base = static_cast<long long>(izr) * a.n_xy;
   const long long e_base = static_cast<long long>(izr) * a.n_rep * nt * nphi;
   __syncthreads();
@@ -381,8 +495,8 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
       const int c = e / n_rot, irot = e % n_rot;
       const int ixy = c0 + c;
       V v = a.psi[(col_base + ixy) * n_rot + irot];
-      v = cscale(cmul(a.before[ir * n_rot + irot], v), oz);
-      if (irot == i0) v = cadd(v, cmul(rot_i0, cmul(a.sp2sc[ixy], incoming)));
+      v = cscale(fmul_t(v, a.before, n_scale, ir * n_rot + irot), oz);
+      if (irot == i0) v = cadd(v, fmul_t(cmul_t(incoming, a.sp2sc, a.n_xy, ixy), a.rot_half, n_scale, ir * n_rot + i0));
       fbr[c * n_rot + irot] = v;
     }
     __syncthreads();
@@ -398,9 +512,9 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
       V s = cmake<V>(0, 0);
       if (blk >= 0) {
         const int nj = a.block_size[blk];
-        const T* row = leg + a.block_offset[blk] + t * nj;
+        const long long r0 = a.block_offset[blk] + t * nj;
         const V* f = fbr + c * n_rot + a.block_first[blk];
-        for (int j = 0; j < nj; ++j) s = cadd(s, cscale(f[j], row[j]));
+        for (int j = 0; j < nj; ++j) s = cadd_scaled(s, f[j], leg[r0 + j], lo_real(leg, n_leg, r0 + j));
       }
       dvr0[c * dvr_col + t * ld + p] = s;
     }
@@ -415,8 +529,8 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
       const int ixy = c0 + c;
       const int rep = a.rep_of[ixy];
       const int pm = a.phi_map[ixy * nphi + p];
-      const V b = a.expia[e_base + (static_cast<long long>(rep) * nt + t) * nphi + pm];
-      cur[c * dvr_col + t * ld + p] = cmul(b, cur[c * dvr_col + t * ld + p]);
+      const long long ei = e_base + (static_cast<long long>(rep) * nt + t) * nphi + pm;
+      cur[c * dvr_col + t * ld + p] = exp_mul(cur[c * dvr_col + t * ld + p], a.expia[ei], a.exp_mod, ei);
     }
     __syncthreads();
     cur = smem_fft(cur, oth, twp, a.pphi, -1, ncol * nt, 1, ld, 1);
@@ -427,10 +541,11 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
       const int nj = a.block_size[blk];
       const int jj = irot - a.block_first[blk];
       const int slot = a.block_slot[blk];
-      const T* col = leg + a.block_offset[blk] + jj;
+      const long long c0l = a.block_offset[blk] + jj;
       V s = cmake<V>(0, 0);
-      for (int t = 0; t < nt; ++t) s = cadd(s, cscale(cur[c * dvr_col + t * ld + slot], col[t * nj]));
-      s = cmul(a.rot_half[ir * n_rot + irot], s);
+      for (int t = 0; t < nt; ++t)
+        s = cadd_scaled(s, cur[c * dvr_col + t * ld + slot], leg[c0l + t * nj], lo_real(leg, n_leg, c0l + t * nj));
+      s = fmul_t(s, a.rot_half, n_scale, ir * n_rot + irot);
       const int ixy = c0 + c;
       if (irot == i0) i0buf[ixy] = s;
       else a.psi[(col_base + ixy) * n_rot + irot] = s;
@@ -440,7 +555,7 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
   // Projection onto the specular grid: a fixed-order sum over (x, y) by warp 0.
   if (threadIdx.x < 32) {
     V s = cmake<V>(0, 0);
-    for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += 32) s = cadd(s, cmul(a.sc2sp[ixy], i0buf[ixy]));
+    for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += 32) s = cadd(s, cmul_t(i0buf[ixy], a.sc2sp, a.n_xy, ixy));
     red[threadIdx.x] = s;
     __syncwarp();
     if (threadIdx.x == 0) {
@@ -453,7 +568,7 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
   __syncthreads();
   const V proj = red[0];
   for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += blockDim.x)
-    a.psi[(col_base + ixy) * n_rot + i0] = csub(i0buf[ixy], cmul(a.sp2sc[ixy], proj));
+    a.psi[(col_base + ixy) * n_rot + i0] = csub(i0buf[ixy], cmul_t(proj, a.sp2sc, a.n_xy, ixy));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -474,20 +589,29 @@ __global__ void gas_phase_kernel(Vec<T>* __restrict__ psi, long long izr_first, 
     const int irot = static_cast<int>(i % n_rot);
     const int ir = static_cast<int>(izr % nr);
     const long long g = izr_first * per_izr + i;
-    psi[g] = cscale(cmul(gas_step[ir * n_rot + irot], psi[g]), opt_z[izr / nr]);
+    psi[g] = cscale(fmul_t(psi[g], gas_step, static_cast<long long>(nr) * n_rot, ir * n_rot + irot), opt_z[izr / nr]);
   }
 }
 
 // exp(i A), A = -V dt, formed in FP64 (src/propagation/potential_operator.cpp:55-65 with
 // src/potential/potential_grid.cpp:164-167), then rounded to T.
 template <typename T>
-__global__ void exp_potential_kernel(const double* __restrict__ v, Vec<T>* __restrict__ out, long long n, double dt) {
+__global__ void exp_potential_kernel(const double* __restrict__ v, Vec<T>* __restrict__ out, __half* __restrict__ mod,
+                                     long long n, double dt) {
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<long long>(gridDim.x) * blockDim.x) {
     const double a = -v[i] * dt;
     double s, c;
     sincos(a, &s, &c);
-    out[i] = cmake<Vec<T>>(static_cast<T>(c), static_cast<T>(s));
+    if constexpr (sizeof(T) == 4) {  // g = exp(i A) - 1 and the modulus correction of 1 + g (see exp_mul)
+      const double cm1 = -2.0 * sin(0.5 * a) * sin(0.5 * a);  // cos A - 1 without cancellation
+      const float gx = static_cast<float>(cm1), gy = static_cast<float>(s);
+      out[i] = cmake<Vec<T>>(gx, gy);
+      const double rx = 1.0 + static_cast<double>(gx), ry = gy;
+      mod[i] = __double2half((1.0 / sqrt(rx * rx + ry * ry) - 1.0) * 16777216.0);
+    } else {
+      out[i] = cmake<Vec<T>>(static_cast<T>(c), static_cast<T>(s));
+    }
   }
 }
 

@@ -18,10 +18,12 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2p_kernel(Axis2Arg
   using V = Vec<T>;
   constexpr int N = N1 * N2;
   constexpr int NS = N1 > N2 ? N1 : N2;
+  constexpr int kParts = sizeof(T) == 4 ? 2 : 1;         // twiddles: value (then low part)
+  constexpr int kFParts = sizeof(T) == 4 ? kFactorParts : 1;  // factors: see fmul_t
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* Y = reinterpret_cast<V*>(smem_raw);
-  V* f = Y + N * TB;
-  V* tw = f + N;
+  V* f = Y + N * TB;       // N factors (the mixed form's parts, see fmul_t)
+  V* tw = f + kFParts * N;  // N twiddles (then N low parts)
   const int b = threadIdx.x % TB;
   const int s = threadIdx.x / TB;
   const long long stride = a.inner;
@@ -39,10 +41,8 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2p_kernel(Axis2Arg
       });
     }
   };
-  for (int k = threadIdx.x; k < N; k += TB * NS) {
-    f[k] = a.factor[k];
-    tw[k] = a.tw[k];
-  }
+  for (int k = threadIdx.x; k < kFParts * N; k += TB * NS) f[k] = a.factor[k];
+  for (int k = threadIdx.x; k < kParts * N; k += TB * NS) tw[k] = a.tw[k];
   __syncthreads();
   long long tile = blockIdx.x, base = 0;
   bool lane_ok = false;
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2p_kernel(Axis2Arg
     if (s < N2) {
       const int n2 = s;
       rdft<N1, -1>(x);
-      static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : cmul(x[k1], tw[n2 * k1]); });
+      static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : tw_mul<N>(x[k1], tw[n2 * k1], lo_part(tw, N, n2 * k1)); });
     }
     __syncthreads();
     // forward level 2, factor, inverse level 2
@@ -73,9 +73,11 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2)) axis2p_kernel(Axis2Arg
       V y[N2];
       static_for<0, N2>([&](auto n2) { y[n2] = Y[(n2 * N1 + k1) * TB + b]; });
       rdft<N2, -1>(y);
-      static_for<0, N2>([&](auto k2) { y[k2] = cmul(f[k1 + N1 * k2], y[k2]); });
+      static_for<0, N2>([&](auto k2) { y[k2] = fmul_t(y[k2], f, N, k1 + N1 * k2); });
       rdft<N2, +1>(y);
-      static_for<0, N2>([&](auto n2) { Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : cmul(y[n2], cconj(tw[n2 * k1])); });
+      static_for<0, N2>([&](auto n2) {
+      Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : tw_mul<N>(y[n2], cconj(tw[n2 * k1]), cconj(lo_part(tw, N, n2 * k1)));
+    });
     }
     __syncthreads();
     // inverse level 1, store
@@ -101,8 +103,9 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2p_kernel(XyArgs<T> 
   using V = Vec<T>;
   constexpr int NXY = NX * NY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kFParts = sizeof(T) == 4 ? kFactorParts : 1;  // the mixed form's factor parts (fmul_t)
   V* S = reinterpret_cast<V*>(smem_raw);  // NXY * TB
-  V* f = S + NXY * TB;                     // NXY
+  V* f = S + NXY * TB;                     // NXY factors (the mixed form's parts)
   const int b = threadIdx.x % TB;
   const int s = threadIdx.x / TB;
   auto locate = [&](long long tile, long long& izr, int& irot, bool& ok) {
@@ -118,7 +121,7 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2p_kernel(XyArgs<T> 
       static_for<0, NY>([&](auto iy) { x[iy] = ok ? a.psi[(col0 + ix * NY + iy) * a.n_rot + irot] : cmake<V>(0, 0); });
     }
   };
-  for (int k = threadIdx.x; k < NXY; k += blockDim.x) f[k] = a.factor[k];
+  for (int k = threadIdx.x; k < kFParts * NXY; k += blockDim.x) f[k] = a.factor[k];
   __syncthreads();
   long long tile = blockIdx.x, izr = 0;
   int irot = 0;
@@ -143,7 +146,7 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2p_kernel(XyArgs<T> 
       const int ix = s;
       if (a.shift_f)
         static_for<0, NY>([&](auto iy) {
-          if (lane_ok) x[iy] = cmul(x[iy], a.shift_f[ix * NY + iy]);
+          if (lane_ok) x[iy] = fmul_t(x[iy], a.shift_f, NXY, ix * NY + iy);
         });
       rdft<NY, -1>(x);
       static_for<0, NY>([&](auto ky) { S[(ix * NY + ky) * TB + b] = x[ky]; });
@@ -154,7 +157,7 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2p_kernel(XyArgs<T> 
       V y[NX];
       static_for<0, NX>([&](auto ix) { y[ix] = S[(ix * NY + ky) * TB + b]; });
       rdft<NX, -1>(y);
-      static_for<0, NX>([&](auto kx) { y[kx] = cmul(f[kx * NY + ky], y[kx]); });
+      static_for<0, NX>([&](auto kx) { y[kx] = fmul_t(y[kx], f, NXY, kx * NY + ky); });
       rdft<NX, +1>(y);
       static_for<0, NX>([&](auto ix) { S[(ix * NY + ky) * TB + b] = y[ix]; });
     }
@@ -166,12 +169,12 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2p_kernel(XyArgs<T> 
       rdft<NY, +1>(z);
       const bool gas = a.apply_gas && izr >= a.izr_gas_first;
       const int ir = static_cast<int>(izr % a.nr);
-      V g = cmake<V>(1, 0);
-      if (gas) g = cscale(a.gas_step[ir * a.n_rot + irot], a.opt_z[izr / a.nr]);
+      const long long n_gas = static_cast<long long>(a.nr) * a.n_rot, k_gas = ir * a.n_rot + irot;
+      const T oz = gas ? a.opt_z[izr / a.nr] : T(1);
       static_for<0, NY>([&](auto iy) {
         V v = z[iy];
-        if (a.shift_b) v = cmul(v, a.shift_b[ix * NY + iy]);
-        if (gas) v = cmul(g, v);
+        if (a.shift_b) v = fmul_t(v, a.shift_b, NXY, ix * NY + iy);
+        if (gas) v = cscale(fmul_t(v, a.gas_step, n_gas, k_gas), oz);
         a.psi[(col0 + ix * NY + iy) * a.n_rot + irot] = v;
       });
     }
@@ -198,20 +201,20 @@ __global__ void __launch_bounds__(TB * N1, sizeof(T) == 4 ? 1024 / (TB * N1) : 1
   using V = Vec<T>;
   static_assert(N2 == 2 * N1, "the balanced form needs N2 = 2 N1");
   constexpr int N = N1 * N2;
+  constexpr int kParts = sizeof(T) == 4 ? 2 : 1;         // twiddles: value (then low part)
+  constexpr int kFParts = sizeof(T) == 4 ? kFactorParts : 1;  // factors: see fmul_t
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* Y = reinterpret_cast<V*>(smem_raw);
-  V* f = Y + N * TB;
-  V* tw = f + N;
+  V* f = Y + N * TB;       // N factors (the mixed form's parts, see fmul_t)
+  V* tw = f + kFParts * N;  // N twiddles (then N low parts)
   const int b = threadIdx.x % TB;
   const int s = threadIdx.x / TB;
   const long long i0 = static_cast<long long>(blockIdx.x) * TB;
   const long long base = static_cast<long long>(blockIdx.y) * N * a.inner + i0 + b;
   const long long stride = a.inner;
   const bool lane_ok = i0 + b < a.inner;
-  for (int k = threadIdx.x; k < N; k += TB * N1) {
-    f[k] = a.factor[k];
-    tw[k] = a.tw[k];
-  }
+  for (int k = threadIdx.x; k < kFParts * N; k += TB * N1) f[k] = a.factor[k];
+  for (int k = threadIdx.x; k < kParts * N; k += TB * N1) tw[k] = a.tw[k];
   __syncthreads();
   // forward, level 1: lines n2 = s, s + N1
 #pragma unroll
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(TB * N1, sizeof(T) == 4 ? 1024 / (TB * N1) : 1
       x[n1] = lane_ok ? a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] : cmake<V>(0, 0);
     });
     rdft<N1, -1>(x);
-    static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : cmul(x[k1], tw[n2 * k1]); });
+    static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : tw_mul<N>(x[k1], tw[n2 * k1], lo_part(tw, N, n2 * k1)); });
   }
   __syncthreads();
   // forward level 2, factor, inverse level 2: line k1 = s
@@ -231,9 +234,11 @@ __global__ void __launch_bounds__(TB * N1, sizeof(T) == 4 ? 1024 / (TB * N1) : 1
     V y[N2];
     static_for<0, N2>([&](auto n2) { y[n2] = Y[(n2 * N1 + k1) * TB + b]; });
     rdft<N2, -1>(y);
-    static_for<0, N2>([&](auto k2) { y[k2] = cmul(f[k1 + N1 * k2], y[k2]); });
+    static_for<0, N2>([&](auto k2) { y[k2] = fmul_t(y[k2], f, N, k1 + N1 * k2); });
     rdft<N2, +1>(y);
-    static_for<0, N2>([&](auto n2) { Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : cmul(y[n2], cconj(tw[n2 * k1])); });
+    static_for<0, N2>([&](auto n2) {
+      Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : tw_mul<N>(y[n2], cconj(tw[n2 * k1]), cconj(lo_part(tw, N, n2 * k1)));
+    });
   }
   __syncthreads();
   // inverse level 1, store: lines n2 = s, s + N1

@@ -163,14 +163,14 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
     auto store_task = [&](int k, V v0, V v1) {
       const int irot = k / PAIRS;
       const int c = 2 * (k - irot * PAIRS);
-      const V b = a.before[ir * n_rot + irot];
-      v0 = c < ncol ? cscale(cmul(b, v0), oz) : cmake<V>(0, 0);
-      v1 = c + 1 < ncol ? cscale(cmul(b, v1), oz) : cmake<V>(0, 0);
+      const long long n_scale = static_cast<long long>(a.nr) * n_rot;  // entries of the scaling tables
+      v0 = c < ncol ? cscale(fmul_t(v0, a.before, n_scale, ir * n_rot + irot), oz) : cmake<V>(0, 0);
+      v1 = c + 1 < ncol ? cscale(fmul_t(v1, a.before, n_scale, ir * n_rot + irot), oz) : cmake<V>(0, 0);
       if (irot == i0) {
         const V incoming = a.chi[izr];
-        const V rot_i0 = a.rot_half[ir * n_rot + i0];
-        if (c < ncol) v0 = cadd(v0, cmul(rot_i0, cmul(a.sp2sc[c0 + c], incoming)));
-        if (c + 1 < ncol) v1 = cadd(v1, cmul(rot_i0, cmul(a.sp2sc[c0 + c + 1], incoming)));
+        if (c < ncol) v0 = cadd(v0, fmul_t(cmul_t(incoming, a.sp2sc, a.n_xy, c0 + c), a.rot_half, n_scale, ir * n_rot + i0));
+        if (c + 1 < ncol)
+          v1 = cadd(v1, fmul_t(cmul_t(incoming, a.sp2sc, a.n_xy, c0 + c + 1), a.rot_half, n_scale, ir * n_rot + i0));
       }
       st2c(F + irot * CB + c, v0, v1);
     };
@@ -244,20 +244,26 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
       static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
       rdft<NPHI, +1>(x);
       if (direct) {
-        if constexpr (EARLY_EXP) static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(e[SPO_CV(p)], x[SPO_CV(p)]); });
+        const long long e0 = ((static_cast<long long>(izr) * a.n_rep + c0 + line_c) * NT + line_t) * NPHI;
+        if constexpr (EARLY_EXP)
+          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = exp_mul(x[SPO_CV(p)], e[SPO_CV(p)], a.exp_mod, e0 + SPO_CV(p)); });
       } else if (g.identity_maps) {
-        const V* ep = a.expia + ((static_cast<long long>(izr) * a.n_rep + ixy) * NT + line_t) * NPHI;
+        const long long e0 = ((static_cast<long long>(izr) * a.n_rep + ixy) * NT + line_t) * NPHI;
+        const V* ep = a.expia + e0;
         static_for<0, NPHI / 2>([&](auto h) {
           constexpr int P = 2 * SPO_CV(h);
-          V e0, e1;
-          ld2c(ep + P, e0, e1);
-          x[P] = cmul(e0, x[P]);
-          x[P + 1] = cmul(e1, x[P + 1]);
+          V ea, eb;
+          ld2c(ep + P, ea, eb);
+          x[P] = exp_mul(x[P], ea, a.exp_mod, e0 + P);
+          x[P + 1] = exp_mul(x[P + 1], eb, a.exp_mod, e0 + P + 1);
         });
       } else {
-        const V* ep = a.expia + ((static_cast<long long>(izr) * a.n_rep + __ldg(a.rep_of + ixy)) * NT + line_t) * NPHI;
+        const long long e0 = ((static_cast<long long>(izr) * a.n_rep + __ldg(a.rep_of + ixy)) * NT + line_t) * NPHI;
         const int* map = a.phi_map + ixy * NPHI;
-        static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(__ldg(ep + __ldg(map + SPO_CV(p))), x[SPO_CV(p)]); });
+        static_for<0, NPHI>([&](auto p) {
+          const long long ei = e0 + __ldg(map + SPO_CV(p));
+          x[SPO_CV(p)] = exp_mul(x[SPO_CV(p)], __ldg(a.expia + ei), a.exp_mod, ei);
+        });
       }
       rdft<NPHI, -1>(x);
       static_for<0, NPHI>([&](auto p) { xl[SPO_CV(p) * SS] = x[SPO_CV(p)]; });
@@ -290,10 +296,11 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
           }
         }
       }
-      const V rh = a.rot_half[ir * n_rot + irot];
+      const long long n_scale = static_cast<long long>(a.nr) * n_rot;
 #pragma unroll
       for (int c = 0; c < CB; ++c)
-        if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, cmake<V>(acc[c][0], acc[c][1]));
+        if (c < ncol)
+          a.psi[(col_base + c) * n_rot + irot] = fmul_t(cmake<V>(acc[c][0], acc[c][1]), a.rot_half, n_scale, ir * n_rot + irot);
     }
   }
 }

@@ -99,8 +99,8 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
 }  // namespace pot5
 
 // Shared memory of potential5_kernel: 2 barriers (padded to 32 bytes), F (CB columns of n_rot + 2
-// values), E (NT CB rows of NPHI + 2 values), X (NPHI padded slot blocks), the scaling rows (one opt_r
-// rot(dt/2) row, two rot(dt/2) rows, CB incoming amplitudes), the matrix rows (n_rot rows of NT + 4),
+// values), E (NT CB rows of NPHI + 2 values), X (NPHI padded slot blocks), the scaling rows with their
+// low parts (one opt_r rot(dt/2) row, two rot(dt/2) rows, CB incoming amplitudes), the matrix rows (n_rot rows of NT + 4),
 // irot -> slot (n_rot ints), the slot sizes and first rows (2 NPHI ints), the schedule (8 sched_len ints).
 // The L2E form keeps neither E nor the opt_r rot(dt/2) row in shared memory.
 template <typename T>
@@ -108,7 +108,7 @@ constexpr std::size_t pot5_smem(int n_rot, int nphi, int nt, int cb, int sched_l
   return 32 + sizeof(Vec<T>) * (static_cast<std::size_t>(cb) * (n_rot + 2) +
                                 (l2e ? 0 : static_cast<std::size_t>(nt) * cb * (nphi + 2)) +
                                 static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb) +
-                                (l2e ? 2 : 3) * static_cast<std::size_t>(n_rot) + cb) +
+                                (l2e ? 4 : 6) * static_cast<std::size_t>(n_rot) + cb) +
          sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) +
          sizeof(int) * (static_cast<std::size_t>(n_rot) + 2 * nphi + 8 * sched_len);
 }
@@ -137,9 +137,10 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
   V* const F = reinterpret_cast<V*>(smem_raw + 32);  // [c][irot], columns of FCS values
   V* E = F + CB * FCS;                     // [line][phi], line = thread (not with L2E)
   V* X = E + (L2E ? 0 : NTH * ERS);        // [p][theta][c], slot blocks of SS values
+  // The scaling rows hold each value and its low part (see cmul2): rows of n_rot values, then n_rot low parts.
   V* Bf = X + NPHI * SS;                   // [irot]: opt_r rot(dt/2) at the item's r point (not with L2E)
-  V* R = Bf + (L2E ? 0 : n_rot);           // [item parity][irot]: rot(dt/2) at the item's r point
-  V* SP = R + 2 * n_rot;                   // [c]: sp2sc(c) * chi, the item's incoming amplitudes
+  V* R = Bf + (L2E ? 0 : 2 * n_rot);       // [item parity][irot]: rot(dt/2) at the item's r point
+  V* SP = R + 4 * n_rot;                   // [c]: sp2sc(c) * chi, the item's incoming amplitudes
   T* L = reinterpret_cast<T*>(SP + CB);    // [irot][position of theta], rows of LDL
   int* irot_slot = reinterpret_cast<int*>(L + n_rot * LDL);
   int* s_nj = irot_slot + n_rot;           // [slot]: J count
@@ -171,8 +172,12 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
   // The item's opt_z value, incoming amplitude chi(point) and (threads c < CB) sp2sc(column c), loaded
   // when the item's copies are issued and used in its scaling phase.
   T oz = 0;
-  V chi_in = cmake<V>(0, 0), sp_in = cmake<V>(0, 0);
+  V chi_in = cmake<V>(0, 0), sp_in = cmake<V>(0, 0), sp_lo = cmake<V>(0, 0);
   V bq[2] = {cmake<V>(0, 0), cmake<V>(0, 0)};  // L2E: opt_r rot(dt/2) of irot tid and tid + NTH
+  V bql[2] = {cmake<V>(0, 0), cmake<V>(0, 0)};  // and their low parts
+  V sb = cmake<V>(1, 0);  // the item's opt_r (and its low part): the scale of its opt_r rot(dt/2) row (fmul_t)
+  const V one = cmake<V>(1, 0);
+  const long long n_scale = static_cast<long long>(a.nr) * n_rot;  // entries of the scaling tables
 
   auto item_columns = [&](long long item, int& izr, int& c0, int& ncol) {
     izr = static_cast<int>(item / g.chunks);
@@ -181,7 +186,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
   };
   // Every thread arrives on each barrier once per phase; the threads that copy announce their bytes.
   // Threads c < ncol copy column c; thread CB the opt_r rot(dt/2) row, thread CB + 1 the rot(dt/2) row
-  // (into R[parity]).
+  // (into R[parity]), CB + 2 its low parts, CB + 3 those of the opt_r rot(dt/2) row.
   auto issue_psi = [&](long long item, int parity_r) {
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
@@ -191,24 +196,36 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       pot5::mbar_arrive_tx(bars, col_bytes + (tid == 0 ? g.extra_tx : 0u));
       pot5::bulk_copy(F + tid * FCS, a.psi + (static_cast<long long>(izr) * a.n_xy + c0 + tid) * n_rot, col_bytes,
                       bars);
-    } else if ((tid == CB && !L2E) || tid == CB + 1) {
+    } else if (((tid == CB || tid == CB + 3) && !L2E) || tid == CB + 1 || tid == CB + 2) {
       pot5::fence_proxy_async();
       pot5::mbar_arrive_tx(bars, col_bytes);
+      const long long row = static_cast<long long>(ir) * n_rot;
       if (tid == CB)
-        pot5::bulk_copy(Bf, a.before + static_cast<long long>(ir) * n_rot, col_bytes, bars);
+        pot5::bulk_copy(Bf, a.before + row, col_bytes, bars);
+      else if (tid == CB + 3)
+        pot5::bulk_copy(Bf + n_rot, a.before + n_scale + row, col_bytes, bars);
+      else if (tid == CB + 1)
+        pot5::bulk_copy(R + parity_r * 2 * n_rot, a.rot_half + row, col_bytes, bars);
       else
-        pot5::bulk_copy(R + parity_r * n_rot, a.rot_half + static_cast<long long>(ir) * n_rot, col_bytes, bars);
+        pot5::bulk_copy(R + parity_r * 2 * n_rot + n_rot, a.rot_half + n_scale + row, col_bytes, bars);
     } else {
       pot5::mbar_arrive(bars);
     }
     if constexpr (L2E) {
 #pragma unroll
       for (int u = 0; u < 2; ++u)
-        if (tid + u * NTH < n_rot) bq[u] = a.before[static_cast<long long>(ir) * n_rot + tid + u * NTH];
+        if (tid + u * NTH < n_rot) {
+          bq[u] = a.before[static_cast<long long>(ir) * n_rot + tid + u * NTH];
+          bql[u] = a.before[n_scale + static_cast<long long>(ir) * n_rot + tid + u * NTH];
+        }
     }
     oz = a.opt_z[izr / a.nr];
+    sb = a.before[2 * n_scale + static_cast<long long>(ir) * n_rot];
     chi_in = a.chi[izr];
-    if (tid < ncol) sp_in = a.sp2sc[c0 + tid];
+    if (tid < ncol) {
+      sp_in = a.sp2sc[c0 + tid];
+      sp_lo = a.sp2sc[a.n_xy + c0 + tid];
+    }
   };
   auto issue_exp = [&](long long item) {
     int izr, c0, ncol;
@@ -217,8 +234,10 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       if (tid < ncol) {
         const int ixy = c0 + tid;
         const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
-        pot5::prefetch_l2(a.expia + (static_cast<long long>(izr) * a.n_rep + rep) * nt_table * NPHI,
-                          static_cast<uint32_t>(nt_table * row_bytes));
+        const long long e0 = (static_cast<long long>(izr) * a.n_rep + rep) * nt_table * NPHI;
+        pot5::prefetch_l2(a.expia + e0, static_cast<uint32_t>(nt_table * row_bytes));
+        // and the rows' modulus corrections (see exp_mul): 2 bytes per entry
+        if ((nt_table * NPHI) % 8 == 0) pot5::prefetch_l2(a.exp_mod + e0, static_cast<uint32_t>(nt_table * NPHI * 2));
       }
       return;
     }
@@ -258,9 +277,9 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
     const long long col_base = static_cast<long long>(izr) * a.n_xy + c0;
-    const V* rh_row = R + rp * n_rot;
+    const V* rh_row = R + rp * 2 * n_rot;  // then its n_rot low parts
     const int ir_item = izr % a.nr;
-    if (tid < CB) SP[tid] = cmul(sp_in, chi_in);  // the previous item's scaling phase has read SP
+    if (tid < CB) SP[tid] = cmul2(chi_in, sp_in, sp_lo);  // the previous item's scaling phase has read SP
 
     // ---- wait for the columns and rows, scale the columns in place (absorbers, rot(dt/2), the
     // specular wave into the initial channel)
@@ -273,18 +292,22 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     // Two rotational states per pass, all their loads before the first store (the compiler cannot tell
     // that the runtime-strided stores to F miss the later loads, and would otherwise serialise them).
     {
-      const V rot_i0 = rh_row[i0];
+      const V rot_i0 = rh_row[i0], rot_i0_lo = rh_row[n_rot + i0];
+      const V sbi = sb;
       for (int ia = tid; ia < n_rot; ia += 2 * NTH) {
         const int ib = ia + NTH;
         const bool has_b = ib < n_rot;
         const int irs[2] = {ia, has_b ? ib : ia};
-        V b[2], v[2][CB];
+        V b[2], bl[2], v[2][CB];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
-          if constexpr (L2E)
+          if constexpr (L2E) {
             b[u] = ia == tid ? bq[u] : a.before[static_cast<long long>(ir_item) * n_rot + irs[u]];
-          else
+            bl[u] = ia == tid ? bql[u] : a.before[n_scale + static_cast<long long>(ir_item) * n_rot + irs[u]];
+          } else {
             b[u] = Bf[irs[u]];
+            bl[u] = Bf[n_rot + irs[u]];
+          }
 #pragma unroll
           for (int c = 0; c < CB; ++c) v[u][c] = F[c * FCS + irs[u]];
         }
@@ -296,8 +319,8 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
           for (int c = 0; c < CB; ++c) {
             V w = cmake<V>(0, 0);
             if (c < ncol) {
-              w = cscale(cmul(b[u], v[u][c]), oz);
-              if (at_i0) w = cadd(w, cmul(rot_i0, SP[c]));  // the specular wave into the initial channel
+              w = cscale(fmul_parts(v[u][c], b[u], bl[u], sbi), oz);
+              if (at_i0) w = cadd(w, fmul_parts(SP[c], rot_i0, rot_i0_lo, one));  // the specular wave into the initial channel
             }
             F[c * FCS + irs[u]] = w;
           }
@@ -351,7 +374,8 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       if (line_c < ncol && line_t < nt_table) {  // padding lines (theta >= nt_table) hold zeros
         const int ixy = c0 + line_c;
         const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
-        const V* eg = a.expia + ((static_cast<long long>(izr) * a.n_rep + rep) * nt_table + line_t) * NPHI;
+        const long long e0 = ((static_cast<long long>(izr) * a.n_rep + rep) * nt_table + line_t) * NPHI;
+        const V* eg = a.expia + e0;
         V* xl = X + line_t * CB + line_c;
         V x[NPHI];
         if (g.identity_maps) {
@@ -364,12 +388,15 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
           });
           static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
           rdft<NPHI, +1>(x);
-          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(e[SPO_CV(p)], x[SPO_CV(p)]); });
+          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = exp_mul(x[SPO_CV(p)], e[SPO_CV(p)], a.exp_mod, e0 + SPO_CV(p)); });
         } else {
           const int* map = a.phi_map + ixy * NPHI;
           static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
           rdft<NPHI, +1>(x);
-          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(eg[__ldg(map + SPO_CV(p))], x[SPO_CV(p)]); });
+          static_for<0, NPHI>([&](auto p) {
+            const int pm = __ldg(map + SPO_CV(p));
+            x[SPO_CV(p)] = exp_mul(x[SPO_CV(p)], eg[pm], a.exp_mod, e0 + pm);
+          });
         }
         rdft<NPHI, -1>(x);
         static_for<0, NPHI>([&](auto p) { xl[SPO_CV(p) * SS] = x[SPO_CV(p)]; });
@@ -385,20 +412,25 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       const int ixy = c0 + line_c;
       V* xl = X + line_t * CB + line_c;
       const V* el = E + tid * ERS;
+      const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
+      const long long e0 = ((static_cast<long long>(izr) * a.n_rep + rep) * nt_table + line_t) * NPHI;
       V x[NPHI];
       static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
       rdft<NPHI, +1>(x);
       if (g.identity_maps) {
         static_for<0, NPHI / 2>([&](auto h) {
           constexpr int P = 2 * SPO_CV(h);
-          V e0, e1;
-          ld2c(el + P, e0, e1);
-          x[P] = cmul(e0, x[P]);
-          x[P + 1] = cmul(e1, x[P + 1]);
+          V ea, eb;
+          ld2c(el + P, ea, eb);
+          x[P] = exp_mul(x[P], ea, a.exp_mod, e0 + P);
+          x[P + 1] = exp_mul(x[P + 1], eb, a.exp_mod, e0 + P + 1);
         });
       } else {
         const int* map = a.phi_map + ixy * NPHI;
-        static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = cmul(el[__ldg(map + SPO_CV(p))], x[SPO_CV(p)]); });
+        static_for<0, NPHI>([&](auto p) {
+          const int pm = __ldg(map + SPO_CV(p));
+          x[SPO_CV(p)] = exp_mul(x[SPO_CV(p)], el[pm], a.exp_mod, e0 + pm);
+        });
       }
       rdft<NPHI, -1>(x);
       static_for<0, NPHI>([&](auto p) { xl[SPO_CV(p) * SS] = x[SPO_CV(p)]; });
@@ -449,10 +481,10 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       for (int u = 0; u < 2; ++u) {
         const int irot = u == 0 ? ia : ib;
         if (u == 1 && !has_b) break;
-        const V rh = rh_row[irot];
+        const V rh = rh_row[irot], rhl = rh_row[n_rot + irot];
 #pragma unroll
         for (int c = 0; c < CB; ++c)
-          if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, cmake<V>(acc[u][c][0], acc[u][c][1]));
+          if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = fmul_parts(cmake<V>(acc[u][c][0], acc[u][c][1]), rh, rhl, one);
       }
     }
   }

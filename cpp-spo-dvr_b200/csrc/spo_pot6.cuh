@@ -146,12 +146,13 @@ constexpr int kPot6RawStride = 64 * 8 + 16;  // bytes per column of a 64-state c
 
 // Shared memory of potential6_kernel (bytes): B forward and transposed (hi, lo), two A stages (hi, lo:
 // 128 rows x 16 K each), two raw chunk buffers (64 columns x 64 states), two opt_r rot(dt/2) rows and two
-// rot(dt/2) rows (item parity), the item's incoming amplitudes, block tables (4 x 32 ints), barriers.
+// rot(dt/2) rows (item parity; each with its low parts, see cmul2), the item's incoming amplitudes, block
+// tables (4 x 32 ints), barriers.
 template <int NT>
 constexpr std::size_t pot6_smem() {
   using B = pot6::Basis<NT>;
   return 4 * 2 * static_cast<std::size_t>(B::kBfFloats + B::kBbFloats) + 2 * 2 * 128 * 16 * 4 +
-         2 * static_cast<std::size_t>(kPot6Tile) * kPot6RawStride + 4 * 8 * static_cast<std::size_t>(B::kRot) +
+         2 * static_cast<std::size_t>(kPot6Tile) * kPot6RawStride + 8 * 8 * static_cast<std::size_t>(B::kRot) +
          8 * kPot6Tile + 4 * 32 * 4 + 64;
 }
 
@@ -174,9 +175,9 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
   float* const bb_s = bf_s + 2 * Bs::kBfFloats;                      // [limb][Bs::kBbFloats]
   unsigned char* const astage = reinterpret_cast<unsigned char*>(bb_s + 2 * Bs::kBbFloats);  // [stage][limb]
   unsigned char* const raw = astage + 2 * 2 * kStageLimb;           // [buffer][column][64 states]
-  V* const before_s = reinterpret_cast<V*>(raw + 2 * kPot6Tile * kPot6RawStride);  // [parity][irot]
-  V* const rot_s = before_s + 2 * NROT;                             // [parity][irot]
-  V* const sp_s = rot_s + 2 * NROT;                                 // [c]: sp2sc(c) chi(point)
+  V* const before_s = reinterpret_cast<V*>(raw + 2 * kPot6Tile * kPot6RawStride);  // [parity][hi, lo][irot]
+  V* const rot_s = before_s + 4 * NROT;                             // [parity][hi, lo][irot]
+  V* const sp_s = rot_s + 4 * NROT;                                 // [c]: sp2sc(c) chi(point)
   int* const tab = reinterpret_cast<int*>(sp_s + kPot6Tile);        // [nj | first | kpad | bf offset][block]
   uint64_t* const bars = reinterpret_cast<uint64_t*>(tab + 4 * 32);  // raw[2], fwd[2], bwd[2]
   uint32_t* const tslot = reinterpret_cast<uint32_t*>(bars + 6);
@@ -228,16 +229,19 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
     item_of(item, izr, c0, ncol);
     const int ir = izr % a.nr;
     const int buf = q & 1;
-    const uint32_t bytes = static_cast<uint32_t>(ncol) * 512u + (q == 0 ? 2u * NROT * 8u : 0u) + g.extra_tx;
+    const uint32_t bytes = static_cast<uint32_t>(ncol) * 512u + (q == 0 ? 4u * NROT * 8u : 0u) + g.extra_tx;
     pot5::fence_proxy_async();
     pot5::mbar_arrive_tx(bar_raw + buf, bytes);
     const V* src = a.psi + (static_cast<long long>(izr) * n_xy + c0) * NROT + 64 * q;
     for (int c = 0; c < ncol; ++c)
       pot5::bulk_copy(raw + (buf * kPot6Tile + c) * kPot6RawStride, src + static_cast<long long>(c) * NROT, 512u,
                       bar_raw + buf);
-    if (q == 0) {
-      pot5::bulk_copy(before_s + rp * NROT, a.before + static_cast<long long>(ir) * NROT, NROT * 8u, bar_raw + buf);
-      pot5::bulk_copy(rot_s + rp * NROT, a.rot_half + static_cast<long long>(ir) * NROT, NROT * 8u, bar_raw + buf);
+    if (q == 0) {  // the rows and their low parts (the n_scale entries after the table)
+      const long long row = static_cast<long long>(ir) * NROT, n_scale = static_cast<long long>(a.nr) * NROT;
+      pot5::bulk_copy(before_s + rp * 2 * NROT, a.before + row, NROT * 8u, bar_raw + buf);
+      pot5::bulk_copy(before_s + rp * 2 * NROT + NROT, a.before + n_scale + row, NROT * 8u, bar_raw + buf);
+      pot5::bulk_copy(rot_s + rp * 2 * NROT, a.rot_half + row, NROT * 8u, bar_raw + buf);
+      pot5::bulk_copy(rot_s + rp * 2 * NROT + NROT, a.rot_half + n_scale + row, NROT * 8u, bar_raw + buf);
     }
   };
   // The item's wave packet (ncol * 2 KB, contiguous) and exp(i A) rows into L2.
@@ -258,8 +262,9 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
     for (int c = lane; c < ncol; c += 32) {
       const int ixy = c0 + c;
       const int rep = g.identity_maps ? ixy : __ldg(a.rep_of + ixy);
-      pot5::prefetch_l2(a.expia + (static_cast<long long>(izr) * a.n_rep + rep) * NT * NPHI,
-                        static_cast<uint32_t>(NT * NPHI * 8));
+      const long long e0 = (static_cast<long long>(izr) * a.n_rep + rep) * NT * NPHI;
+      pot5::prefetch_l2(a.expia + e0, static_cast<uint32_t>(NT * NPHI * 8));
+      pot5::prefetch_l2(a.exp_mod + e0, static_cast<uint32_t>(NT * NPHI * 2));
     }
   };
   // A bounded wait by every thread on bars[k]; true for the whole block when one of them gave up.
@@ -295,7 +300,11 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
     if (warp == 0) prefetch_exp(item);
     if (warp == 1 && next < g.n_items) prefetch_psi(next);
     const float oz = a.opt_z[izr / a.nr];
-    if (tid < kPot6Tile) sp_s[tid] = tid < ncol ? cmul(a.sp2sc[c0 + tid], a.chi[izr]) : make_float2(0.f, 0.f);
+    // the item's opt_r (and its low part), the scale of its opt_r rot(dt/2) row (see fmul_t)
+    const V sb = a.before[2 * static_cast<long long>(a.nr) * NROT + static_cast<long long>(izr % a.nr) * NROT];
+    const V one = make_float2(1.f, 0.f);
+    if (tid < kPot6Tile)
+      sp_s[tid] = tid < ncol ? cmul2(a.chi[izr], a.sp2sc[c0 + tid], a.sp2sc[n_xy + c0 + tid]) : make_float2(0.f, 0.f);
     uint32_t waited = 0;  // raw chunks of this item already waited for
 
     // ------------------------------------------------------------------ forward contraction
@@ -324,8 +333,9 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
             const int qq = irot >> 6;
             const V v = *reinterpret_cast<const V*>(raw + ((qq & 1) * kPot6Tile + st_c) * kPot6RawStride +
                                                     (irot & 63) * 8);
-            w[e] = cscale(cmul(before_s[rp * NROT + irot], v), oz);
-            if (irot == i0) w[e] = cadd(w[e], cmul(rot_s[rp * NROT + i0], sp_s[st_c]));
+            w[e] = cscale(fmul_parts(v, before_s[rp * 2 * NROT + irot], before_s[rp * 2 * NROT + NROT + irot], sb), oz);
+            if (irot == i0)
+              w[e] = cadd(w[e], fmul_parts(sp_s[st_c], rot_s[rp * 2 * NROT + i0], rot_s[rp * 2 * NROT + NROT + i0], one));
           }
         }
         // exchange: comp 0 keeps the real parts (its quad, and the partner's), comp 1 the imaginary parts
@@ -401,8 +411,10 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
       for (int pp = 0; pp < 4; ++pp) {
         const int th0 = 8 * half + 2 * pp;   // the pair's two lines: theta th0 (comp 0) and th0 + 1 (comp 1)
         const int th = th0 + t_comp;        // this thread's line
-        const V* eg = a.expia + ((static_cast<long long>(izr) * a.n_rep + rep) * NT + th) * NPHI;
+        const long long e0 = ((static_cast<long long>(izr) * a.n_rep + rep) * NT + th) * NPHI;
+        const V* eg = a.expia + e0;
         V e[NPHI];
+        float em[NPHI];  // the entries' modulus corrections (see exp_mul)
         if (valid && g.identity_maps) {
 #pragma unroll
           for (int h = 0; h < NPHI / 2; ++h) {
@@ -410,13 +422,22 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
             e[2 * h] = make_float2(qv.x, qv.y);
             e[2 * h + 1] = make_float2(qv.z, qv.w);
           }
+#pragma unroll
+          for (int h = 0; h < NPHI; ++h) em[h] = __half2float(__ldg(a.exp_mod + e0 + h)) * 5.9604644775390625e-8f;
         } else if (valid) {
           const int* map = a.phi_map + ixy * NPHI;
 #pragma unroll
-          for (int h = 0; h < NPHI; ++h) e[h] = __ldg(eg + __ldg(map + h));
+          for (int h = 0; h < NPHI; ++h) {
+            const int pm = __ldg(map + h);
+            e[h] = __ldg(eg + pm);
+            em[h] = __half2float(__ldg(a.exp_mod + e0 + pm)) * 5.9604644775390625e-8f;
+          }
         } else {
 #pragma unroll
-          for (int h = 0; h < NPHI; ++h) e[h] = make_float2(0.f, 0.f);
+          for (int h = 0; h < NPHI; ++h) {
+            e[h] = make_float2(0.f, 0.f);
+            em[h] = 0.f;
+          }
         }
         uint32_t v0[NB], v1[NB];
 #pragma unroll
@@ -434,7 +455,8 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
         }
         rdft<NPHI, +1>(x);
 #pragma unroll
-        for (int p = 0; p < NPHI; ++p) x[p] = cmul(e[p], x[p]);
+        for (int p = 0; p < NPHI; ++p)  // x (1 + g)(1 + m), g the table entry (see exp_mul)
+          x[p] = cadd(x[p], cmul2(x[p], e[p], make_float2(em[p] * (1.0f + e[p].x), em[p] * e[p].y)));
         rdft<NPHI, -1>(x);
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
@@ -453,7 +475,7 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
     pot6::fence_after_sync();
 
     // ------------------------------------------------------------------ transposed contraction
-    const V* rot_row = rot_s + rp * NROT;
+    const V* rot_row = rot_s + rp * 2 * NROT;  // then its NROT low parts
     auto epilogue = [&](int b) {
       // the slot's 16 J columns (comp part) of this thread's lane, J = 8 half .. + 7
       uint32_t u[8];
@@ -468,7 +490,7 @@ __global__ void __launch_bounds__(kPot6Threads, 1) potential6_kernel(Pot6Args<fl
         // comp 0: J = 8 half + 2 s2 (Re ev, Im recv); comp 1: J + 1 (Re recv, Im od)
         const int j = 8 * half + 2 * s2 + t_comp;
         const V y = t_comp ? make_float2(recv, od) : make_float2(ev, recv);
-        if (j < nj && t_c < ncol) out[j] = cmul(rot_row[first + j], y);
+        if (j < nj && t_c < ncol) out[j] = fmul_parts(y, rot_row[first + j], rot_row[NROT + first + j], one);
       }
     };
     for (int b = 0; b < NB && !failed; ++b) {

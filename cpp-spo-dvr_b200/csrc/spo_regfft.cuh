@@ -94,8 +94,27 @@ SPO_HD V twiddle_mul(V a) {
     using R = decltype(V::x);
     constexpr R c = static_cast<R>(Root<k, N, S>::re);
     constexpr R s = static_cast<R>(Root<k, N, S>::im);
-    return cmake<V>(a.x * c - a.y * s, a.x * s + a.y * c);
+    if constexpr (sizeof(R) == 4 && (N & (N - 1)) != 0) {
+      // mixed form, roots of lengths with an odd factor: the product in FP64, rounded once (with FP32
+      // partial sums these roots drift the norm of a pass by ~2e-9, the same sign every pass)
+      constexpr double cd = Root<k, N, S>::re, sd = Root<k, N, S>::im;
+      const double ax = a.x, ay = a.y;
+      return cmake<V>(static_cast<R>(ax * cd - ay * sd), static_cast<R>(ax * sd + ay * cd));
+    } else if constexpr (sizeof(R) == 4) {  // mixed form: the root as c + cl, s + sl (see cmul2)
+      constexpr R cl = static_cast<R>(Root<k, N, S>::re - static_cast<double>(c));
+      constexpr R sl = static_cast<R>(Root<k, N, S>::im - static_cast<double>(s));
+      return cmul2(a, cmake<V>(c, s), cmake<V>(cl, sl));
+    } else {
+      return cmake<V>(a.x * c - a.y * s, a.x * s + a.y * c);
+    }
   }
+}
+
+// A runtime twiddle of a length-N transform: FP64 product for lengths with an odd factor, else cmul2.
+template <int N, typename V>
+SPO_HD V tw_mul(V a, V w, V wl) {
+  if constexpr ((N & (N - 1)) != 0) return cmul_dd(a, w, wl);
+  else return cmul2(a, w, wl);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -132,7 +151,11 @@ SPO_HD void rdft(V (&x)[N]) {
     x[3] = csub(d02, jd);
   } else if constexpr (N == 3 || N == 5 || N == 7 || N == 11) {
     // Odd prime: pairs (t, N - t) share the real part of the root and have opposite imaginary parts.
+    // The mixed form sums each output pair in FP64 from the FP32 sums and differences and rounds once: summed
+    // in FP32, the shared partial sums of the pair drift the norm of a forward-inverse pass with a phase
+    // between them by ~2e-8 (radix 3), the same sign every pass.
     using R = decltype(V::x);
+    using A = std::conditional_t<sizeof(R) == 4, double, R>;  // accumulation type
     constexpr int H = N / 2;
     V s[H + 1], d[H + 1];
     static_for<1, H + 1>([&](auto t) {
@@ -144,19 +167,18 @@ SPO_HD void rdft(V (&x)[N]) {
     static_for<1, H + 1>([&](auto t) { o0 = cadd(o0, s[t]); });
     out[0] = o0;
     static_for<1, H + 1>([&](auto q) {
-      V re = x[0];
-      R ir = 0, ii = 0;
+      A rex = x[0].x, rey = x[0].y, ir = 0, ii = 0;
       static_for<1, H + 1>([&](auto t) {
         constexpr long tq = static_cast<long>(SPO_CV(t)) * SPO_CV(q) % N;
-        constexpr R c = static_cast<R>(Root<tq, N, S>::re);
-        constexpr R sn = static_cast<R>(Root<tq, N, S>::im);
-        re = cmake<V>(re.x + c * s[t].x, re.y + c * s[t].y);
-        ir += sn * d[t].x;
-        ii += sn * d[t].y;
+        constexpr A c = static_cast<A>(Root<tq, N, S>::re);
+        constexpr A sn = static_cast<A>(Root<tq, N, S>::im);
+        rex += c * static_cast<A>(s[t].x);
+        rey += c * static_cast<A>(s[t].y);
+        ir += sn * static_cast<A>(d[t].x);
+        ii += sn * static_cast<A>(d[t].y);
       });
-      const V rot = cmake<V>(-ii, ir);  // i * sum Im(w) d
-      out[q] = cadd(re, rot);
-      out[N - q] = csub(re, rot);
+      out[q] = cmake<V>(static_cast<R>(rex - ii), static_cast<R>(rey + ir));  // re + i * sum Im(w) d
+      out[N - q] = cmake<V>(static_cast<R>(rex + ii), static_cast<R>(rey - ir));
     });
     static_for<0, N>([&](auto t) { x[t] = out[t]; });
   } else {
@@ -220,10 +242,12 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2), sizeof(T) == 4 && (N1 
   using V = Vec<T>;
   constexpr int N = N1 * N2;
   constexpr int NS = N1 > N2 ? N1 : N2;
+  constexpr int kParts = sizeof(T) == 4 ? 2 : 1;         // twiddles: value (then low part)
+  constexpr int kFParts = sizeof(T) == 4 ? kFactorParts : 1;  // factors: see fmul_t
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* Y = reinterpret_cast<V*>(smem_raw);
-  V* f = Y + N * TB;
-  V* tw = f + N;
+  V* f = Y + N * TB;       // N factors (the mixed form's parts, see fmul_t)
+  V* tw = f + kFParts * N;  // N twiddles (then N low parts)
   const int b = threadIdx.x % TB;
   const int s = threadIdx.x / TB;
   long long base, stride;
@@ -240,10 +264,8 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2), sizeof(T) == 4 && (N1 
     stride = a.line_stride;
     lane_ok = in_group < a.window;
   }
-  for (int k = threadIdx.x; k < N; k += TB * NS) {
-    f[k] = a.factor[k];
-    tw[k] = a.tw[k];
-  }
+  for (int k = threadIdx.x; k < kFParts * N; k += TB * NS) f[k] = a.factor[k];
+  for (int k = threadIdx.x; k < kParts * N; k += TB * NS) tw[k] = a.tw[k];
   __syncthreads();
   // forward, level 1
   if (s < N2) {
@@ -253,7 +275,7 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2), sizeof(T) == 4 && (N1 
       x[n1] = lane_ok ? a.data[base + static_cast<long long>(n2 + N2 * n1) * stride] : cmake<V>(0, 0);
     });
     rdft<N1, -1>(x);
-    static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : cmul(x[k1], tw[n2 * k1]); });
+    static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = k1 == 0 ? x[k1] : tw_mul<N>(x[k1], tw[n2 * k1], lo_part(tw, N, n2 * k1)); });
   }
   __syncthreads();
   // forward level 2, factor, inverse level 2
@@ -262,9 +284,11 @@ __global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2), sizeof(T) == 4 && (N1 
     V y[N2];
     static_for<0, N2>([&](auto n2) { y[n2] = Y[(n2 * N1 + k1) * TB + b]; });
     rdft<N2, -1>(y);
-    static_for<0, N2>([&](auto k2) { y[k2] = cmul(f[k1 + N1 * k2], y[k2]); });
+    static_for<0, N2>([&](auto k2) { y[k2] = fmul_t(y[k2], f, N, k1 + N1 * k2); });
     rdft<N2, +1>(y);
-    static_for<0, N2>([&](auto n2) { Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : cmul(y[n2], cconj(tw[n2 * k1])); });
+    static_for<0, N2>([&](auto n2) {
+      Y[(n2 * N1 + k1) * TB + b] = n2 == 0 ? y[n2] : tw_mul<N>(y[n2], cconj(tw[n2 * k1]), cconj(lo_part(tw, N, n2 * k1)));
+    });
   }
   __syncthreads();
   // inverse level 1, store
@@ -294,15 +318,16 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2_kernel(XyArgs<T> a
   using V = Vec<T>;
   constexpr int NXY = NX * NY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kFParts = sizeof(T) == 4 ? kFactorParts : 1;  // the mixed form's factor parts (fmul_t)
   V* S = reinterpret_cast<V*>(smem_raw);  // NXY * TB
-  V* f = S + NXY * TB;                     // NXY
+  V* f = S + NXY * TB;                     // NXY factors (the mixed form's parts)
   const int b = threadIdx.x % TB;
   const int s = threadIdx.x / TB;
   const long long izr = a.izr_offset + blockIdx.y;
   const int irot = blockIdx.x * TB + b;
   const bool lane_ok = irot < a.n_rot;
   const long long col0 = izr * NXY;
-  for (int k = threadIdx.x; k < NXY; k += blockDim.x) f[k] = a.factor[k];
+  for (int k = threadIdx.x; k < kFParts * NXY; k += blockDim.x) f[k] = a.factor[k];
   if (s < NX) {
     const int ix = s;
     V x[NY];
@@ -310,7 +335,7 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2_kernel(XyArgs<T> a
       V v = cmake<V>(0, 0);
       if (lane_ok) {
         v = a.psi[(col0 + ix * NY + iy) * a.n_rot + irot];
-        if (a.shift_f) v = cmul(v, a.shift_f[ix * NY + iy]);
+        if (a.shift_f) v = fmul_t(v, a.shift_f, NXY, ix * NY + iy);
       }
       x[iy] = v;
     });
@@ -323,7 +348,7 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2_kernel(XyArgs<T> a
     V x[NX];
     static_for<0, NX>([&](auto ix) { x[ix] = S[(ix * NY + ky) * TB + b]; });
     rdft<NX, -1>(x);
-    static_for<0, NX>([&](auto kx) { x[kx] = cmul(f[kx * NY + ky], x[kx]); });
+    static_for<0, NX>([&](auto kx) { x[kx] = fmul_t(x[kx], f, NXY, kx * NY + ky); });
     rdft<NX, +1>(x);
     static_for<0, NX>([&](auto ix) { S[(ix * NY + ky) * TB + b] = x[ix]; });
   }
@@ -335,12 +360,12 @@ __global__ void __launch_bounds__(TB*(NX > NY ? NX : NY)) xy2_kernel(XyArgs<T> a
     rdft<NY, +1>(x);
     const bool gas = a.apply_gas && izr >= a.izr_gas_first;
     const int ir = static_cast<int>(izr % a.nr);
-    V g = cmake<V>(1, 0);
-    if (gas) g = cscale(a.gas_step[ir * a.n_rot + irot], a.opt_z[izr / a.nr]);
+    const long long n_gas = static_cast<long long>(a.nr) * a.n_rot, k_gas = ir * a.n_rot + irot;
+    const T oz = gas ? a.opt_z[izr / a.nr] : T(1);
     static_for<0, NY>([&](auto iy) {
       V v = x[iy];
-      if (a.shift_b) v = cmul(v, a.shift_b[ix * NY + iy]);
-      if (gas) v = cmul(g, v);
+      if (a.shift_b) v = fmul_t(v, a.shift_b, NXY, ix * NY + iy);
+      if (gas) v = cscale(fmul_t(v, a.gas_step, n_gas, k_gas), oz);
       a.psi[(col0 + ix * NY + iy) * a.n_rot + irot] = v;
     });
   }
@@ -387,16 +412,17 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
   V* D = F + CB * n_rot;                  // CB * nt * LD
   V* i0buf = D + CB * nt * LD;            // n_xy
   V* red = i0buf + a.n_xy;                // 32
-  T* leg = reinterpret_cast<T*>(red + 32);  // nt * n_rot, (block, theta, J)
+  T* leg = reinterpret_cast<T*>(red + 32);  // nt * n_rot, (block, theta, J) (then, mixed form, their low parts)
+  const long long n_leg = static_cast<long long>(nt) * n_rot;
   const int izr = blockIdx.x;
   const int ir = izr % a.nr;
   const int iz = izr / a.nr;
   const int i0 = a.initial_channel;
   const int mj_max = a.mj_max;
-  for (int k = threadIdx.x; k < nt * n_rot; k += blockDim.x) leg[k] = a.legendre[k];
+  for (int k = threadIdx.x; k < (sizeof(T) == 4 ? 2 : 1) * nt * n_rot; k += blockDim.x) leg[k] = a.legendre[k];
   const T oz = a.opt_z[iz];
   const V incoming = a.chi[ir + a.nr * iz];
-  const V rot_i0 = a.rot_half[ir * n_rot + i0];
+  const long long n_scale = static_cast<long long>(a.nr) * n_rot;  // entries of the scaling tables
   const long long col_base = static_cast<long long>(izr) * a.n_xy;
   const long long e_base = static_cast<long long>(izr) * a.n_rep * nt * NPHI;
   const int line_c = threadIdx.x / nt;  // this thread's line: column line_c, theta line_t
@@ -409,8 +435,8 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
       const int c = e / n_rot, irot = e - c * n_rot;
       const int ixy = c0 + c;
       V v = a.psi[(col_base + ixy) * n_rot + irot];
-      v = cscale(cmul(a.before[ir * n_rot + irot], v), oz);
-      if (irot == i0) v = cadd(v, cmul(rot_i0, cmul(a.sp2sc[ixy], incoming)));
+      v = cscale(fmul_t(v, a.before, n_scale, ir * n_rot + irot), oz);
+      if (irot == i0) v = cadd(v, fmul_t(cmul_t(incoming, a.sp2sc, a.n_xy, ixy), a.rot_half, n_scale, ir * n_rot + i0));
       F[c * n_rot + irot] = v;
     }
     __syncthreads();
@@ -427,23 +453,25 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
           const int blk = mj_max + m;
           const int nj = a.block_size[blk];
           const int first = a.block_first[blk];
-          const T* mt = args.legendre_t + a.block_offset[blk] + t;  // (J, theta) within the block
+          const long long m0 = a.block_offset[blk] + t;  // (J, theta) within the block
           for (int j = 0; j < nj; ++j) {
-            const T w = __ldg(mt + j * nt);
-            const V fv = f[first + j];
-            s = cmake<V>(s.x + w * fv.x, s.y + w * fv.y);
+            const long long k = m0 + j * nt;
+            s = cadd_scaled(s, f[first + j], __ldg(args.legendre_t + k), lo_real(args.legendre_t, n_leg, k));
           }
         }
         x[P] = s;
       });
       rdft<NPHI, +1>(x);
       if (args.identity_maps) {
-        const V* e = a.expia + e_base + (static_cast<long long>(ixy) * nt + t) * NPHI;
-        static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + p), x[p]); });
+        const long long e0 = e_base + (static_cast<long long>(ixy) * nt + t) * NPHI;
+        static_for<0, NPHI>([&](auto p) { x[p] = exp_mul(x[p], __ldg(a.expia + e0 + p), a.exp_mod, e0 + p); });
       } else {
-        const V* e = a.expia + e_base + (static_cast<long long>(a.rep_of[ixy]) * nt + t) * NPHI;
+        const long long e0 = e_base + (static_cast<long long>(a.rep_of[ixy]) * nt + t) * NPHI;
         const int* map = a.phi_map + ixy * NPHI;
-        static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + __ldg(map + p)), x[p]); });
+        static_for<0, NPHI>([&](auto p) {
+          const long long ei = e0 + __ldg(map + p);
+          x[p] = exp_mul(x[p], __ldg(a.expia + ei), a.exp_mod, ei);
+        });
       }
       rdft<NPHI, -1>(x);
       static_for<0, NPHI>([&](auto p) { D[(c * nt + t) * LD + p] = x[p]; });
@@ -454,24 +482,20 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
       const int nj = a.block_size[blk];
       const int jj = irot - a.block_first[blk];
       const int slot = a.block_slot[blk];
-      const T* col = leg + a.block_offset[blk] + jj;
+      const long long c0l = a.block_offset[blk] + jj;
       V acc[CB];
 #pragma unroll
       for (int c = 0; c < CB; ++c) acc[c] = cmake<V>(0, 0);
       for (int t = 0; t < nt; ++t) {
-        const T w = col[t * nj];
+        const T w = leg[c0l + t * nj], wl = lo_real(leg, n_leg, c0l + t * nj);
         const V* d = D + t * LD + slot;
 #pragma unroll
-        for (int c = 0; c < CB; ++c) {
-          const V dv = d[c * nt * LD];
-          acc[c] = cmake<V>(acc[c].x + w * dv.x, acc[c].y + w * dv.y);
-        }
+        for (int c = 0; c < CB; ++c) acc[c] = cadd_scaled(acc[c], d[c * nt * LD], w, wl);
       }
-      const V rh = a.rot_half[ir * n_rot + irot];
 #pragma unroll
       for (int c = 0; c < CB; ++c) {
         if (c < ncol) {
-          const V s = cmul(rh, acc[c]);
+          const V s = fmul_t(acc[c], a.rot_half, n_scale, ir * n_rot + irot);
           if (irot == i0) i0buf[c0 + c] = s;
           else a.psi[(col_base + c0 + c) * n_rot + irot] = s;
         }
@@ -481,7 +505,7 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
   }
   if (threadIdx.x < 32) {
     V s = cmake<V>(0, 0);
-    for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += 32) s = cadd(s, cmul(a.sc2sp[ixy], i0buf[ixy]));
+    for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += 32) s = cadd(s, cmul_t(i0buf[ixy], a.sc2sp, a.n_xy, ixy));
     red[threadIdx.x] = s;
     __syncwarp();
     if (threadIdx.x == 0) {
@@ -494,7 +518,7 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
   __syncthreads();
   const V proj = red[0];
   for (int ixy = threadIdx.x; ixy < a.n_xy; ixy += blockDim.x)
-    a.psi[(col_base + ixy) * n_rot + i0] = csub(i0buf[ixy], cmul(a.sp2sc[ixy], proj));
+    a.psi[(col_base + ixy) * n_rot + i0] = csub(i0buf[ixy], cmul_t(proj, a.sp2sc, a.n_xy, ixy));
 }
 
 }  // namespace spo
@@ -545,10 +569,11 @@ __global__ void __launch_bounds__(CB * 16) potential3_kernel(Pot2Args<T> args) {
     if (j < __ldg(args.slot_nj + p)) {
       const int irot = __ldg(args.slot_first + p) + j;
       v = a.psi[(col_base + c) * n_rot + irot];
-      v = cscale(cmul(a.before[ir * n_rot + irot], v), oz);
+      const long long n_scale = static_cast<long long>(a.nr) * n_rot;  // entries of the scaling tables
+      v = cscale(fmul_t(v, a.before, n_scale, ir * n_rot + irot), oz);
       if (irot == i0) {
         const V incoming = a.chi[ir + a.nr * iz];
-        v = cadd(v, cmul(a.rot_half[ir * n_rot + i0], cmul(a.sp2sc[c0 + c], incoming)));
+        v = cadd(v, fmul_t(cmul_t(incoming, a.sp2sc, a.n_xy, c0 + c), a.rot_half, n_scale, ir * n_rot + i0));
       }
     }
     F[c * FS + r] = v;
@@ -561,13 +586,13 @@ __global__ void __launch_bounds__(CB * 16) potential3_kernel(Pot2Args<T> args) {
   if (has_line) {
     const V* f = F + line_c * FS;
     const T* mt = args.legendre_slot + line_t;
+    const long long n_slot = static_cast<long long>(NPHI) * jp * nt;  // low parts follow (mixed form)
     static_for<0, NPHI>([&](auto p) { x[p] = cmake<V>(0, 0); });
     for (int j = 0; j < jp; ++j) {
       static_for<0, NPHI>([&](auto p) {
         constexpr int P = SPO_CV(p);
-        const T w = __ldg(mt + (P * jp + j) * nt);
-        const V fv = f[P * jp + j];
-        x[P] = cmake<V>(x[P].x + w * fv.x, x[P].y + w * fv.y);
+        const long long k = (P * jp + j) * nt;
+        x[P] = cadd_scaled(x[P], f[P * jp + j], __ldg(mt + k), lo_real(mt, n_slot, k));
       });
     }
   }
@@ -576,12 +601,15 @@ __global__ void __launch_bounds__(CB * 16) potential3_kernel(Pot2Args<T> args) {
     const int ixy = c0 + line_c;
     rdft<NPHI, +1>(x);
     if (args.identity_maps) {
-      const V* e = a.expia + (static_cast<long long>(izr) * a.n_rep + ixy) * nt * NPHI + line_t * NPHI;
-      static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + p), x[p]); });
+      const long long e0 = (static_cast<long long>(izr) * a.n_rep + ixy) * nt * NPHI + line_t * NPHI;
+      static_for<0, NPHI>([&](auto p) { x[p] = exp_mul(x[p], __ldg(a.expia + e0 + p), a.exp_mod, e0 + p); });
     } else {
-      const V* e = a.expia + (static_cast<long long>(izr) * a.n_rep + a.rep_of[ixy]) * nt * NPHI + line_t * NPHI;
+      const long long e0 = (static_cast<long long>(izr) * a.n_rep + a.rep_of[ixy]) * nt * NPHI + line_t * NPHI;
       const int* map = a.phi_map + ixy * NPHI;
-      static_for<0, NPHI>([&](auto p) { x[p] = cmul(__ldg(e + __ldg(map + p)), x[p]); });
+      static_for<0, NPHI>([&](auto p) {
+        const long long ei = e0 + __ldg(map + p);
+        x[p] = exp_mul(x[p], __ldg(a.expia + ei), a.exp_mod, ei);
+      });
     }
     rdft<NPHI, -1>(x);
     static_for<0, NPHI>([&](auto p) { D[(line_c * nt + line_t) * LD + p] = x[p]; });
@@ -593,22 +621,20 @@ __global__ void __launch_bounds__(CB * 16) potential3_kernel(Pot2Args<T> args) {
     const int jj = irot - __ldg(a.block_first + blk);
     const int slot = __ldg(a.block_slot + blk);
     const T* col = a.legendre + __ldg(a.block_offset + blk) + jj;  // (theta, J) within the block
+    const long long n_leg = static_cast<long long>(nt) * n_rot;      // low parts follow (mixed form)
     V acc[CB];
 #pragma unroll
     for (int c = 0; c < CB; ++c) acc[c] = cmake<V>(0, 0);
     for (int t = 0; t < nt; ++t) {
-      const T w = __ldg(col + t * nj);
+      const T w = __ldg(col + t * nj), wl = lo_real(col, n_leg, t * nj);
       const V* d = D + t * LD + slot;
 #pragma unroll
-      for (int c = 0; c < CB; ++c) {
-        const V dv = d[c * nt * LD];
-        acc[c] = cmake<V>(acc[c].x + w * dv.x, acc[c].y + w * dv.y);
-      }
+      for (int c = 0; c < CB; ++c) acc[c] = cadd_scaled(acc[c], d[c * nt * LD], w, wl);
     }
-    const V rh = a.rot_half[ir * n_rot + irot];
+    const long long n_scale = static_cast<long long>(a.nr) * n_rot;
 #pragma unroll
     for (int c = 0; c < CB; ++c)
-      if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = cmul(rh, acc[c]);
+      if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = fmul_t(acc[c], a.rot_half, n_scale, ir * n_rot + irot);
   }
 }
 
@@ -628,15 +654,26 @@ __global__ void projection_finalize_kernel(Vec<T>* __restrict__ psi, Vec<T>* __r
   for (int ixy = threadIdx.x; ixy < n_xy; ixy += blockDim.x) col[ixy] = psi[(base + ixy) * n_rot + i0];
   __syncthreads();
   if (threadIdx.x == 0) {
-    V p = cmake<V>(0, 0);
-    for (int ixy = 0; ixy < n_xy; ++ixy) p = cadd(p, cmul(sc2sp[ixy], col[ixy]));
-    proj = p;
-    chi[blockIdx.x] = p;
+    if constexpr (sizeof(T) == 4) {  // mixed form: the sum in FP64, the coefficients with their low parts
+      double px = 0.0, py = 0.0;
+      for (int ixy = 0; ixy < n_xy; ++ixy) {
+        const V w = sc2sp[ixy], wl = sc2sp[n_xy + ixy], v = col[ixy];
+        const double wx = static_cast<double>(w.x) + wl.x, wy = static_cast<double>(w.y) + wl.y;
+        px += wx * v.x - wy * v.y;
+        py += wx * v.y + wy * v.x;
+      }
+      proj = cmake<V>(static_cast<T>(px), static_cast<T>(py));
+    } else {
+      V p = cmake<V>(0, 0);
+      for (int ixy = 0; ixy < n_xy; ++ixy) p = cadd(p, cmul(sc2sp[ixy], col[ixy]));
+      proj = p;
+    }
+    chi[blockIdx.x] = proj;
   }
   __syncthreads();
   const V p = proj;
   for (int ixy = threadIdx.x; ixy < n_xy; ixy += blockDim.x)
-    psi[(base + ixy) * n_rot + i0] = csub(col[ixy], cmul(sp2sc[ixy], p));
+    psi[(base + ixy) * n_rot + i0] = csub(col[ixy], cmul_t(p, sp2sc, n_xy, ixy));
 }
 
 }  // namespace spo

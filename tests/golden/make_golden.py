@@ -25,7 +25,7 @@ import sys
 
 import numpy as np
 
-CASES = {"hardwall_short": 10, "cu111_dailight_short": 5, "cu111_dailight_oblique": 5}
+CASES = {"hardwall_short": 10, "cu111_dailight_short": 5, "cu111_dailight_oblique": 5, "cu111_dailight_small": 50}
 
 
 def fortran_records(path):

@@ -7,7 +7,7 @@ compiled from its sources), with the reference GPU tests' LCG wave packet over t
 analysis step (5 time steps). The same case bundle and packet then go through the C ABI:
   - nX = nY = 16 is the benchmark's grid itself: the FP64 form runs the kernels the FP64 line times
     (axis2b<128>, axis2<48>, xy2p<16>, potential4<32,16>), the mixed form those of the headline
-    (potential6<32,16>: both theta contractions as split-precision TF32 tcgen05 GEMMs);
+    (potential5<32,16> with exp(i A) rows through L2);
   - nX = nY = 4 runs the same Z, r and potential kernels on a smaller (x, y) grid.
 Bars: the FP64 bar (relative L2 1e-10) and the mixed form's 3e-5, on psi and chi.
 """
@@ -55,5 +55,5 @@ def test_config2_analysis_step_matches_oracle(ref_case, tmp_path, nx):
             if precision == "fp64":
                 assert "potential4<nphi=32,nt=16" in kernels and "xy2p<16" in kernels, kernels
             else:
-                assert "potential6<nphi=32,nt=16" in kernels, kernels
+                assert "potential5<nphi=32,nt=16" in kernels, kernels
         del psi
