@@ -242,6 +242,24 @@ def reference_timing(analysis_steps: int, warmup: int, nx: int = 4):
     return out, None
 
 
+PRECISION_RECORD = os.path.join(ROOT, "tests", "golden", "precision_config3.json")
+
+
+def precision_record():
+    """The committed record of the precision form's error on this workload (tests/golden/precision_config3.py:
+    configuration 2 and 3 through the reference program with the B200 backend, 20000 steps, 81 energies)."""
+    try:
+        with open(PRECISION_RECORD) as f:
+            r = json.load(f)
+    except (OSError, ValueError):
+        return None
+    return {"dP_reaction": r["dp_reaction_max"], "dP_state_max": r["dp_state_max"],
+            "bar": 1e-6, "time_steps": r["time_steps"], "energies": r["energies"],
+            "open_channels": r["open_channels"],
+            "source": "tests/golden/precision_config3.json: configuration 2 (FP64) and 3 (mixed) through the "
+                      "reference program with the B200 backend (oracle/_ref/spodvr_b200), 20000 time steps"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -430,6 +448,11 @@ def main():
             "gpu_launches": m["launches"],
             "clocks": m["clocks"],
         }
+        prec = precision_record()
+        if prec is not None and args.workload == "config3":
+            line["dP_reaction"] = prec["dP_reaction"]
+            line["dP_state_max"] = prec["dP_state_max"]
+            line["precision"] = prec
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -169,6 +169,33 @@ int spo_profile_entry(const spo_handle* h, int i, char* name, int name_len, doub
   return SPO_OK;
 }
 
+int spo_norm_budget_setup(spo_handle* h, const spo_norm_budget_desc* d, int* n_absorbers) {
+  return guarded(h, [&] {
+    require(d != nullptr && n_absorbers != nullptr, "spo_norm_budget_setup: null pointer");
+    require(d->volume_scattering > 0.0 && d->volume_specular > 0.0, "spo_norm_budget_setup: volumes must be positive");
+    require((d->z_low_first < 0 || (d->z_low_first <= d->z_low_last && d->z_low_last < h->s.nz)) &&
+                (d->zs_low_first < 0 || (d->zs_low_first <= d->zs_low_last && d->zs_low_last < h->s.nzs)),
+            "spo_norm_budget_setup: low absorber range out of the grid");
+    *n_absorbers = h->impl->norm_budget_setup(*d);
+  });
+}
+
+int spo_norm_budget_add(spo_handle* h, double* loss, double* loss_error, double* norms, int* has_window) {
+  return guarded(h, [&] {
+    require(loss && loss_error && norms && has_window, "spo_norm_budget_add: null pointer");
+    double out[2 * spo::kBudgetMaxAbsorbers + 2];
+    *has_window = h->impl->norm_budget_add(out) ? 1 : 0;
+    if (!*has_window) return;
+    const int n = h->impl->norm_budget_absorbers();
+    for (int a = 0; a < n; ++a) {
+      loss[a] = out[a];
+      loss_error[a] = out[n + a];
+    }
+    norms[0] = out[2 * n];
+    norms[1] = out[2 * n + 1];
+  });
+}
+
 int spo_test_wait_timeout(spo_handle* h, int poll_limit, int unmatched_bytes) {
   if (h && (unmatched_bytes < 0 || unmatched_bytes % 16 != 0 || unmatched_bytes > 4096)) {
     h->err = "spo_test_wait_timeout: unmatched_bytes must be a multiple of 16 in [0, 4096]";

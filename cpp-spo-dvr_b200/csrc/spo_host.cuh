@@ -238,7 +238,7 @@ bool launch_axis2(int n, const spo::Axis2Args<T>& a, long long outer, cudaStream
     case 24: return launch_axis2_n<T, 4, 6>(a, outer, stream);
     case 32: return launch_axis2_n<T, 4, 8>(a, outer, stream);
     case 40: return launch_axis2_n<T, 5, 8>(a, outer, stream);
-    case 48: return launch_axis2_n<T, 3, 16>(a, outer, stream);  // the odd factor in the first level only
+    case 48: return launch_axis2_n<T, 6, 8>(a, outer, stream);
     case 56: return launch_axis2_n<T, 7, 8>(a, outer, stream);
     case 64: return launch_axis2_n<T, 8, 8>(a, outer, stream);
     case 80: return launch_axis2_n<T, 8, 10>(a, outer, stream);
@@ -607,6 +607,9 @@ class StepBase {
   virtual void set_stream(cudaStream_t s) = 0;
   virtual void profile(bool on) = 0;
   virtual void set_wait_test(int poll_limit, unsigned extra_bytes) = 0;
+  virtual int norm_budget_setup(const spo_norm_budget_desc& d) = 0;
+  virtual bool norm_budget_add(double* out) = 0;
+  virtual int norm_budget_absorbers() const = 0;
   virtual const std::vector<KernelRecord>& records() const = 0;
 };
 
@@ -720,6 +723,95 @@ class Step final : public StepBase {
     check_cuda(cudaMemcpyAsync(out, densities_, sizeof(double) * s_.n_zr(), cudaMemcpyDeviceToHost, stream_),
                "block_densities copy");
     check_cuda(cudaStreamSynchronize(stream_), "block_densities");
+  }
+
+  // The norm budget's absorption of every cell of both grids, as NormBudget's constructor
+  // (src/analysis/norm_budget.cpp:39-71): absorbers ZOpt, [ZOptLow], ROpt (scattering), ZSpOpt, [ZSpOptLow],
+  // ROpt (specular); per cell the window exponent 2 n V_opt dt, the Z absorber and its share of the loss
+  // (V_opt,Z / (V_opt,Z + V_opt,r)), the r absorber. Returns the number of absorbers.
+  int norm_budget_setup(const spo_norm_budget_desc& d) override {
+    int n_abs = 0;
+    const int z_opt = n_abs++;
+    const int z_opt_low = d.z_low_first >= 0 ? n_abs++ : -1;
+    const int r_opt = n_abs++;
+    const int zsp_opt = n_abs++;
+    const int zsp_opt_low = d.zs_low_first >= 0 ? n_abs++ : -1;
+    const int r_opt_spec = n_abs++;
+    auto absorption = [&](const std::vector<double>& zf, int z_high, int z_low, int low_first, int low_last,
+                          int r_index, spo::BudgetGrid& g, std::vector<double>& exponent, std::vector<double>& share,
+                          std::vector<int>& za, std::vector<int>& ra) {
+      const std::size_t cells = zf.size() * static_cast<std::size_t>(s_.nr);
+      exponent.assign(cells, 0.0);
+      share.assign(cells, 0.0);
+      za.assign(cells, -1);
+      ra.assign(cells, -1);
+      for (int iz = 0; iz < static_cast<int>(zf.size()); ++iz)
+        for (int ir = 0; ir < s_.nr; ++ir) {
+          const double v_z = -std::log(zf[iz]), v_r = -std::log(host_opt_r_[ir]);
+          if (v_z == 0.0 && v_r == 0.0) continue;
+          const std::size_t k = ir + static_cast<std::size_t>(s_.nr) * iz;
+          exponent[k] = 2.0 * s_.spa * (v_z + v_r);
+          if (v_z != 0.0) {
+            za[k] = (low_first >= 0 && iz >= low_first && iz <= low_last) ? z_low : z_high;
+            share[k] = v_z / (v_z + v_r);
+          }
+          if (v_r != 0.0) ra[k] = r_index;
+        }
+      g.cells = static_cast<long long>(cells);
+    };
+    std::vector<double> e0, s0, e1, s1;
+    std::vector<int> za0, ra0, za1, ra1;
+    absorption(host_opt_z_, z_opt, z_opt_low, d.z_low_first, d.z_low_last, r_opt, budget_scat_, e0, s0, za0, ra0);
+    absorption(host_opt_zs_, zsp_opt, zsp_opt_low, d.zs_low_first, d.zs_low_last, r_opt_spec, budget_spec_, e1, s1,
+               za1, ra1);
+    auto up_d = [&](const std::vector<double>& v) {
+      double* p = dev<double>(v.size());
+      check_cuda(cudaMemcpy(p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice), "norm budget tables");
+      return p;
+    };
+    auto up_i = [&](const std::vector<int>& v) {
+      int* p = dev<int>(v.size());
+      check_cuda(cudaMemcpy(p, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice), "norm budget tables");
+      return p;
+    };
+    budget_scat_.exponent = up_d(e0);
+    budget_scat_.z_share = up_d(s0);
+    budget_scat_.z_absorber = up_i(za0);
+    budget_scat_.r_absorber = up_i(ra0);
+    budget_scat_.previous = dev<double>(e0.size());
+    budget_spec_.exponent = up_d(e1);
+    budget_spec_.z_share = up_d(s1);
+    budget_spec_.z_absorber = up_i(za1);
+    budget_spec_.r_absorber = up_i(ra1);
+    budget_spec_.previous = dev<double>(e1.size());
+    budget_out_ = dev<double>(2 * spo::kBudgetMaxAbsorbers + 2);
+    budget_abs_ = n_abs;
+    budget_vol_scat_ = d.volume_scattering;
+    budget_vol_spec_ = d.volume_specular;
+    budget_has_previous_ = false;
+    return n_abs;
+  }
+
+  int norm_budget_absorbers() const override { return budget_abs_; }
+
+  // One window of the norm budget (NormBudget::add, src/analysis/norm_budget.cpp:100-112) from the resident
+  // state: out = losses (n_absorbers), loss errors (n_absorbers), norm at the window's start and end. False (out
+  // untouched) at the first call, which only records the cells.
+  bool norm_budget_add(double* out) override {
+    require(budget_abs_ > 0, "spo_norm_budget_add: spo_norm_budget_setup was not called");
+    spo::block_density_kernel<T><<<static_cast<unsigned>(s_.n_zr()), 256, 0, stream_>>>(
+        psi_, s_.n_xy() * s_.n_rot, densities_);
+    spo::norm_budget_kernel<T><<<1, 256, 0, stream_>>>(densities_, budget_vol_scat_, chi_, budget_vol_spec_,
+                                                      budget_scat_, budget_spec_, budget_abs_,
+                                                      budget_has_previous_ ? 1 : 0, budget_out_);
+    check_cuda(cudaGetLastError(), "norm budget launch");
+    const bool window = budget_has_previous_;
+    if (window)
+      check_cuda(cudaMemcpyAsync(out, budget_out_, sizeof(double) * (2 * budget_abs_ + 2), cudaMemcpyDeviceToHost,
+                                 stream_), "norm budget copy");
+    check_cuda(cudaStreamSynchronize(stream_), "norm budget");
+    budget_has_previous_ = true;
+    return window;
   }
 
   void averages(const double* z, const double* zs, const double* r, double vol_scat, double vol_spec, int iz_analysis,
@@ -1357,6 +1449,9 @@ class Step final : public StepBase {
     const std::vector<double> opt_r = real_array(d.r_optical, s.nr, "r_optical");
     const std::vector<double> opt_z = real_array(d.z_optical, s.nz, "z_optical");
     const std::vector<double> opt_zs = real_array(d.z_specular_optical, s.nzs, "z_specular_optical");
+    host_opt_z_ = opt_z;
+    host_opt_r_ = opt_r;
+    host_opt_zs_ = opt_zs;
     const std::vector<cplx> gas = complex_array(d.gas_phase, s.nr, "gas_phase");
     std::vector<cplx> before(rot.size()), gas_step(rot.size());
     for (int ir = 0; ir < s.nr; ++ir)
@@ -1462,8 +1557,10 @@ class Step final : public StepBase {
     const long long n_e = s.n_expia();
     require(d.potential != nullptr || n_e == 0, "potential is null");
     // The mixed form keeps, after the n_e table entries, their n_e modulus corrections (FP16, spo::exp_mul).
-    expia_ = dev<V>(std::max<long long>(n_e + (sizeof(T) == 4 ? (n_e + 3) / 4 : 0), 1));
-    __half* exp_mod = sizeof(T) == 4 ? reinterpret_cast<__half*>(expia_ + n_e) : nullptr;
+    // (from a 16-byte boundary: the kernels read 8 corrections per load and prefetch rows of them into L2)
+    const long long n_e_even = (n_e + 1) & ~1ll;
+    expia_ = dev<V>(std::max<long long>(n_e_even + (sizeof(T) == 4 ? (n_e + 3) / 4 : 0), 1));
+    __half* exp_mod = sizeof(T) == 4 ? reinterpret_cast<__half*>(expia_ + n_e_even) : nullptr;
     double* vstage = reinterpret_cast<double*>(staging_);
     const long long chunk = 2 * staging_elems_;
     for (long long i = 0; i < n_e; i += chunk) {
@@ -1868,6 +1965,13 @@ class Step final : public StepBase {
   std::size_t pot5_smem_ = 0;
   bool pot5_l2e_ = false;  // potential5's L2E form (exp(i A) rows through L2, three blocks per SM)
   int* error_flag_ = nullptr;  // set by a kernel whose bounded wait gave up
+  // the norm budget (norm_budget_setup / norm_budget_add) and the FP64 absorber factors it is built from
+  std::vector<double> host_opt_z_, host_opt_r_, host_opt_zs_;
+  spo::BudgetGrid budget_scat_{}, budget_spec_{};
+  double* budget_out_ = nullptr;
+  int budget_abs_ = 0;
+  double budget_vol_scat_ = 0.0, budget_vol_spec_ = 0.0;
+  bool budget_has_previous_ = false;
   int pot_kind_ = 1;  // 1 general, 2 potential2, 3 potential3, 4 potential4, 5 potential5, 6 potential6
   // potential6: both theta contractions on the tensor cores (mixed form, nphi 32, ntheta 16, square basis)
   spo::Pot6Args<float> pot6_args_{};

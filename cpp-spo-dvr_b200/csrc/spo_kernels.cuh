@@ -98,15 +98,24 @@ __device__ __forceinline__ V cadd_scaled(V s, V f, decltype(V::x) w, decltype(V:
 // fmul_t) and, per entry, m = 1/|1 + g| - 1 (FP16, a multiple of 2^-24): x (1 + g)(1 + m) = x + x (g + m (1 + g)).
 // Without m a point's norm would change by |1 + g|^2 - 1 (~1e-8) every step, for all points of equal V the same
 // way. The FP64 form holds exp(i A) itself.
+// The same with the correction given: m as stored (a multiple of 2^-24 times 2^24) in FP32.
 template <typename V>
-__device__ __forceinline__ V exp_mul(V x, V e, const __half* mod, long long idx) {
+__device__ __forceinline__ V exp_mul_m(V x, V e, float m24) {
   if constexpr (sizeof(V) == 8) {
-    const float m = __half2float(__ldg(mod + idx)) * 5.9604644775390625e-8f;  // 2^-24
+    const float m = m24 * 5.9604644775390625e-8f;  // 2^-24
     return cadd(x, cmul2(x, e, make_float2(m * (1.0f + e.x), m * e.y)));
   } else {
     return cmul(e, x);
   }
 }
+template <typename V>
+__device__ __forceinline__ V exp_mul(V x, V e, const __half* mod, long long idx) {
+  if constexpr (sizeof(V) == 8) return exp_mul_m(x, e, __half2float(__ldg(mod + idx)));
+  else return cmul(e, x);
+}
+// The corrections of entries 2i and 2i + 1 of a row read as 32-bit words (one __half2 per word).
+__device__ __forceinline__ float mod_lo(uint32_t w) { return __low2float(*reinterpret_cast<const __half2*>(&w)); }
+__device__ __forceinline__ float mod_hi(uint32_t w) { return __high2float(*reinterpret_cast<const __half2*>(&w)); }
 
 // x times entry k of a factor table: a factor s e^{i phi} with s >= 0 real (a kinetic or rotation phase, with an
 // FFT scale or an absorber). The mixed form holds each factor as g = e^{i phi} - 1 (n values), the low parts of g
@@ -612,6 +621,91 @@ __global__ void exp_potential_kernel(const double* __restrict__ v, Vec<T>* __res
     } else {
       out[i] = cmake<Vec<T>>(static_cast<T>(c), static_cast<T>(s));
     }
+  }
+}
+
+// The norm budget of one analysis window on the device, FP64 (src/analysis/norm_budget.cpp:24-35, 75-111):
+// the cell probabilities of the current state (block densities times the scattering cell volume, |chi|^2 times
+// the specular one), the loss of every absorbing cell over the window from the previous call's cells
+//   gamma = window exponent, F = exp(-gamma), 1 - F = -expm1(-gamma),
+//   loss = rho_start (1 - F) + (rho_end - F rho_start) (gamma / (1 - F) - 1),
+//   error = gamma^2 / 6 |rho_end - rho_start + loss|,
+// shared between the cell's Z absorber (z_share) and its r absorber (the rest), and the norms at the window's
+// start and end. One block, a fixed assignment of cells to threads and a fixed tree: the sums are repeatable
+// (not in the reference's serial order; they agree to rounding). The current cells replace the previous ones.
+constexpr int kBudgetMaxAbsorbers = 6;
+struct BudgetGrid {
+  const double* exponent;  // per cell: 2 n V_opt dt of the window (0: the cell does not absorb)
+  const double* z_share;   // per cell: the Z absorber's share of the loss
+  const int* z_absorber;   // per cell: index of the Z absorber, -1: none
+  const int* r_absorber;   // per cell: index of the r absorber, -1: none
+  double* previous;        // the cells of the previous call
+  long long cells;
+};
+template <typename T>
+__global__ void __launch_bounds__(256) norm_budget_kernel(const double* __restrict__ densities, double vol_scat,
+                                                          const Vec<T>* __restrict__ chi, double vol_spec,
+                                                          BudgetGrid scat, BudgetGrid spec, int n_absorbers,
+                                                          int has_previous, double* __restrict__ out) {
+  constexpr int NV = 2 * kBudgetMaxAbsorbers + 2;  // loss, error per absorber; norm at start, at end
+  __shared__ double part[NV][256];
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  for (int grid = 0; grid < 2; ++grid) {
+    const BudgetGrid& g = grid == 0 ? scat : spec;
+    for (long long k = threadIdx.x; k < g.cells; k += blockDim.x) {
+      double rho_end;
+      if (grid == 0) {
+        rho_end = densities[k] * vol_scat;
+      } else {
+        const Vec<T> c = chi[k];
+        rho_end = (static_cast<double>(c.x) * c.x + static_cast<double>(c.y) * c.y) * vol_spec;
+      }
+      if (has_previous) {
+        const double rho_start = g.previous[k];
+        acc[NV - 2] += rho_start;
+        acc[NV - 1] += rho_end;
+        const int za = g.z_absorber[k], ra = g.r_absorber[k];
+        if (za >= 0 || ra >= 0) {
+          const double gamma = g.exponent[k];
+          const double one_minus_f = -expm1(-gamma);
+          const double f = exp(-gamma);
+          const double loss = rho_start * one_minus_f + (rho_end - f * rho_start) * (gamma / one_minus_f - 1.0);
+          const double err = gamma * gamma / 6.0 * fabs(rho_end - rho_start + loss);
+          const double zs = g.z_share[k];
+#pragma unroll
+          for (int a = 0; a < kBudgetMaxAbsorbers; ++a) {
+            if (a == za) {
+              acc[a] += zs * loss;
+              acc[kBudgetMaxAbsorbers + a] += zs * err;
+            }
+            if (a == ra) {
+              acc[a] += (1.0 - zs) * loss;
+              acc[kBudgetMaxAbsorbers + a] += (1.0 - zs) * err;
+            }
+          }
+        }
+      }
+      g.previous[k] = rho_end;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NV; ++k) part[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) part[k][threadIdx.x] += part[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int a = 0; a < n_absorbers; ++a) {
+      out[a] = part[a][0];
+      out[n_absorbers + a] = part[kBudgetMaxAbsorbers + a][0];
+    }
+    out[2 * n_absorbers] = part[NV - 2][0];
+    out[2 * n_absorbers + 1] = part[NV - 1][0];
   }
 }
 

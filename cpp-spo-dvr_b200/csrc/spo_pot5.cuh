@@ -386,9 +386,27 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
             e[P] = cmake<V>(q.x, q.y);
             e[P + 1] = cmake<V>(q.z, q.w);
           });
-          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
-          rdft<NPHI, +1>(x);
-          static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = exp_mul(x[SPO_CV(p)], e[SPO_CV(p)], a.exp_mod, e0 + SPO_CV(p)); });
+          if constexpr (sizeof(T) == 4 && NPHI % 8 == 0) {  // the row's corrections, 16 bytes per load
+            uint32_t mw[NPHI / 2];
+            static_for<0, NPHI / 8>([&](auto h) {
+              const uint4 q = __ldg(reinterpret_cast<const uint4*>(a.exp_mod + e0) + SPO_CV(h));
+              mw[4 * SPO_CV(h)] = q.x;
+              mw[4 * SPO_CV(h) + 1] = q.y;
+              mw[4 * SPO_CV(h) + 2] = q.z;
+              mw[4 * SPO_CV(h) + 3] = q.w;
+            });
+            static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
+            rdft<NPHI, +1>(x);
+            static_for<0, NPHI / 2>([&](auto h) {
+              constexpr int P = 2 * SPO_CV(h);
+              x[P] = exp_mul_m(x[P], e[P], mod_lo(mw[SPO_CV(h)]));
+              x[P + 1] = exp_mul_m(x[P + 1], e[P + 1], mod_hi(mw[SPO_CV(h)]));
+            });
+          } else {
+            static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });
+            rdft<NPHI, +1>(x);
+            static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = exp_mul(x[SPO_CV(p)], e[SPO_CV(p)], a.exp_mod, e0 + SPO_CV(p)); });
+          }
         } else {
           const int* map = a.phi_map + ixy * NPHI;
           static_for<0, NPHI>([&](auto p) { x[SPO_CV(p)] = xl[SPO_CV(p) * SS]; });

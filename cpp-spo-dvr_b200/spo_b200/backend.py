@@ -194,6 +194,27 @@ class B200Backend:
         """Run on the caller's cudaStream_t (an integer handle, e.g. torch.cuda.Stream().cuda_stream)."""
         self._check(self._lib.spo_set_stream(self._h, ctypes.c_void_p(cuda_stream or 0)))
 
+    def norm_budget_setup(self, volume_scattering: float, volume_specular: float, z_low=None, zs_low=None) -> int:
+        """The norm budget's tables on the device (NormBudget's constructor); returns the number of absorbers.
+        z_low / zs_low: (first, last) of the low-Z absorber of each grid, or None."""
+        d = capi.NormBudgetDesc(z_low[0] if z_low else -1, z_low[1] if z_low else -1,
+                                zs_low[0] if zs_low else -1, zs_low[1] if zs_low else -1,
+                                volume_scattering, volume_specular)
+        n = ctypes.c_int(0)
+        self._check(self._lib.spo_norm_budget_setup(self._h, ctypes.byref(d), ctypes.byref(n)))
+        self._budget_absorbers = n.value
+        return n.value
+
+    def norm_budget_add(self):
+        """NormBudget::add on the resident state: None at the first call, else (loss, loss_error, norm_start,
+        norm_end) of the window since the previous call."""
+        n = self._budget_absorbers
+        loss, err, norms = np.zeros(n), np.zeros(n), np.zeros(2)
+        has = ctypes.c_int(0)
+        self._check(self._lib.spo_norm_budget_add(self._h, capi.dptr(loss), capi.dptr(err), capi.dptr(norms),
+                                                  ctypes.byref(has)))
+        return (loss, err, float(norms[0]), float(norms[1])) if has.value else None
+
     def test_wait_timeout(self, poll_limit: int, unmatched_bytes: int) -> None:
         """Failure-detection test of the bounded device waits (spo_test_wait_timeout): the potential kernel's
         barriers expect unmatched_bytes more than their copies deliver and give up after poll_limit polls;

@@ -31,7 +31,8 @@ EXPORTS = [
     "spo_profile_count", "spo_profile_entry", "spo_device_bytes", "spo_last_launch_count",
     "spo_block_densities_noalloc", "spo_analysis_setup", "spo_bk_coefficients", "spo_s_matrix_sums",
     "spo_describe", "spo_averages", "spo_ensemble_create", "spo_ensemble_step", "spo_ensemble_launch_count",
-    "spo_ensemble_last_error", "spo_ensemble_destroy", "spo_test_wait_timeout",
+    "spo_ensemble_last_error", "spo_ensemble_destroy", "spo_test_wait_timeout", "spo_norm_budget_setup",
+    "spo_norm_budget_add",
 ]
 NOALLOC_MAX_BLOCKS = 65536
 
@@ -75,6 +76,13 @@ class SpoAnalysisDesc(ctypes.Structure):
     ]
 
 
+class NormBudgetDesc(ctypes.Structure):
+    """struct spo_norm_budget_desc of include/spo_b200.h."""
+    _fields_ = [("z_low_first", ctypes.c_int), ("z_low_last", ctypes.c_int), ("zs_low_first", ctypes.c_int),
+                ("zs_low_last", ctypes.c_int), ("volume_scattering", ctypes.c_double),
+                ("volume_specular", ctypes.c_double)]
+
+
 class B200Error(RuntimeError):
     """A non-zero status of the C ABI, with the library's message."""
 
@@ -108,6 +116,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.spo_profile_entry.argtypes = [h, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, _dp, _ip, _dp]
     lib.spo_device_bytes.argtypes = [h, ctypes.POINTER(ctypes.c_ulonglong)]
     lib.spo_test_wait_timeout.argtypes = [h, ctypes.c_int, ctypes.c_int]
+    lib.spo_norm_budget_setup.argtypes = [h, ctypes.POINTER(NormBudgetDesc), _ip]
+    lib.spo_norm_budget_add.argtypes = [h, _dp, _dp, _dp, _ip]
     lib.spo_analysis_setup.argtypes = [h, ctypes.POINTER(SpoAnalysisDesc)]
     lib.spo_bk_coefficients.argtypes = [h, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
     lib.spo_s_matrix_sums.argtypes = [h, _dp]

@@ -246,6 +246,30 @@ int spo_averages(spo_handle* h, const double* z, const double* z_specular, const
                  double volume_specular, int iz_analysis, int surface_index, double* out);
 
 /* ---------------------------------------------------------------------------------------------
+ * The norm budget on the device, in FP64 whatever the precision form: per analysis window, the probability
+ * each absorber removed (NormBudget, src/analysis/norm_budget.hpp:45-84). The absorbers and their cells come
+ * from the handle's absorber factors (spo_desc z_optical, r_optical, z_specular_optical) as NormBudget's
+ * constructor builds them (norm_budget.cpp:39-71): ZOpt, [ZOptLow], ROpt (scattering grid), ZSpOpt,
+ * [ZSpOptLow], ROpt (specular grid), the bracketed ones only when their Z range is given.
+ * --------------------------------------------------------------------------------------------- */
+typedef struct spo_norm_budget_desc {
+  int z_low_first, z_low_last;    /* SpatialGrids::z_optical_low (inclusive), or -1, -1 */
+  int zs_low_first, zs_low_last;  /* SpatialGrids::z_specular_optical_low, or -1, -1 */
+  double volume_scattering;       /* dZ dr times the (x, y) volume element (cell_probabilities, averages.cpp:85-97) */
+  double volume_specular;         /* dZ dr */
+} spo_norm_budget_desc;
+
+/* Builds the budget's tables on the device; *n_absorbers receives their number (4 to 6). Replaces the
+ * NormBudget constructor (norm_budget.cpp:39-50). */
+int spo_norm_budget_setup(spo_handle* h, const spo_norm_budget_desc* d, int* n_absorbers);
+
+/* The window that ends at the resident state and starts at the state of the previous call (NormBudget::add,
+ * norm_budget.cpp:100-112): *has_window = 0 at the first call (nothing written); otherwise loss and loss_error
+ * (n_absorbers values each, in the absorber order above) and norms[0], norms[1] (the probability on both grids
+ * at the window's start and end). Cell sums in a fixed order on the device. */
+int spo_norm_budget_add(spo_handle* h, double* loss, double* loss_error, double* norms, int* has_window);
+
+/* ---------------------------------------------------------------------------------------------
  * Ensembles of wave packets (no counterpart in the reference, which propagates one wave packet per
  * run): one analysis step of every member handle, captured once as one CUDA graph with one branch per
  * member, so that one graph launch advances all of them and members of uneven grid sizes overlap on
