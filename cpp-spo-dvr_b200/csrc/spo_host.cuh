@@ -1221,19 +1221,21 @@ class Step final : public StepBase {
       if (std::string(env) == "0") return;
     constexpr int reps = 3;
     const double b = 0.0;
+    // Each width is timed in two interleaved rounds after one untimed round of all three (the GPU's clock
+    // may still be rising when a handle is created), and keeps its faster round.
     auto choose = [&](int& tile, auto&& run) {
-      int best = 16;
-      tile = 16;
-      float best_ms = time_launches(run, reps);
-      for (const int t : {8, 32}) {
-        tile = t;
-        const float ms = time_launches(run, reps);
-        if (ms < 0.98f * best_ms) {  // another width only when clearly faster
-          best = t;
-          best_ms = ms;
+      constexpr int widths[3] = {16, 8, 32};
+      float ms[3] = {0.0f, 0.0f, 0.0f};
+      for (int round = 0; round < 3; ++round)
+        for (int k = 0; k < 3; ++k) {
+          tile = widths[k];
+          const float t = time_launches(run, reps);
+          if (round == 1 || (round == 2 && t < ms[k])) ms[k] = t;
         }
-      }
-      tile = best;
+      int best = 0;
+      for (int k = 1; k < 3; ++k)
+        if (ms[k] < 0.98f * ms[best]) best = k;  // another width only when clearly faster
+      tile = widths[best];
     };
     const bool was_on = prof_.on();
     prof_.enable(false);

@@ -53,15 +53,42 @@ SPO_HD float2 cmul2(float2 a, float2 w, float2 wl) {
 SPO_HD double2 cmul2(double2 a, double2 w, double2) {
   return make_double2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
 }
-// a * (w + wl) as one FP64 product rounded once (mixed form). Twiddles of transform lengths with an odd
-// factor (48 = 3 x 16, ...) need it: with FP32 partial sums their products still drift the norm of a pass
-// by ~1e-9, the same sign every pass; powers of two do not (cmul2 suffices).
-SPO_HD float2 cmul_dd(float2 a, float2 w, float2 wl) {
-  const double wx = static_cast<double>(w.x) + wl.x, wy = static_cast<double>(w.y) + wl.y;
-  const double ax = a.x, ay = a.y;
-  return make_float2(static_cast<float>(ax * wx - ay * wy), static_cast<float>(ax * wy + ay * wx));
+// FP32 products and sums that the compiler may not fuse into FMAs (an error-free transformation needs the
+// rounded product and the rounded sum themselves).
+SPO_HD float mul_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fmul_rn(a, b);
+#else
+  return a * b;
+#endif
 }
-SPO_HD double2 cmul_dd(double2 a, double2 w, double2) {
+SPO_HD float add_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+// a b + c d + tl, nearly correctly rounded, in FP32 only: each product split exactly into its rounding and
+// its error by an FMA (TwoProduct), the two roundings added with the error of the sum kept (Knuth's
+// TwoSum), the errors and tl added last (the compensated dot product of Ogita, Rump and Oishi, "Accurate
+// sum and dot product", SIAM J. Sci. Comput. 26, 2005).
+SPO_HD float dot2_comp(float a, float b, float c, float d, float tl) {
+  const float p1 = mul_rn(a, b), e1 = fmaf(a, b, -p1);
+  const float p2 = mul_rn(c, d), e2 = fmaf(c, d, -p2);
+  const float s = add_rn(p1, p2), bb = add_rn(s, -p1);
+  const float es = add_rn(add_rn(p1, -add_rn(s, -bb)), add_rn(p2, -bb));
+  return add_rn(s, add_rn(add_rn(es, e1), add_rn(e2, tl)));
+}
+// a * (w + wl) with each component nearly correctly rounded (mixed form). Twiddles of transform lengths with
+// an odd factor (48 = 6 x 8, ...) need it: rounded as cmul2 rounds, their products drift the norm of a
+// forward-inverse pass by ~2.6e-9, the same sign every pass (powers of two do not: cmul2 suffices); summed
+// this way the drift is ~1e-11, as with an FP64 product, without the conversions.
+SPO_HD float2 cmul_comp(float2 a, float2 w, float2 wl) {
+  return make_float2(dot2_comp(a.x, w.x, -a.y, w.y, fmaf(a.x, wl.x, -a.y * wl.y)),
+                     dot2_comp(a.x, w.y, a.y, w.x, fmaf(a.x, wl.y, a.y * wl.x)));
+}
+SPO_HD double2 cmul_comp(double2 a, double2 w, double2) {
   return make_double2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
 }
 
@@ -87,11 +114,24 @@ __device__ __forceinline__ T lo_real(const T* table, long long n, long long k) {
   if constexpr (sizeof(T) == 4) return table[n + k];
   else return T(0);
 }
-// s + w f for a real matrix entry held as w + wl (mixed form; the small term first).
+// Accumulators of the small-grid potential kernels' theta contractions: FP64 in both forms. The mixed form's
+// matrix entry w + wl enters as one FP64 value and the sum is rounded to FP32 once (acc_out). Summed in FP32,
+// the low part wl is mostly lost (it lies below half an ulp of the running sum), and the round trip of the
+// forward and the transposed contraction then gains ~1.4e-8 of the norm per step on a physical wave packet
+// whose rotational phases turn (host emulation of these kernels on cu111_dailight_small); summed in FP64,
+// ~1e-10.
+template <typename V> struct AccOf { using type = double2; };
+template <typename V> using Acc = typename AccOf<V>::type;
+__device__ __forceinline__ double2 acc_zero() { return make_double2(0.0, 0.0); }
+// s + (w + wl) f
 template <typename V>
-__device__ __forceinline__ V cadd_scaled(V s, V f, decltype(V::x) w, decltype(V::x) wl) {
-  if constexpr (sizeof(V) == 8) return cmake<V>(fmaf(w, f.x, fmaf(wl, f.x, s.x)), fmaf(w, f.y, fmaf(wl, f.y, s.y)));
-  else return cmake<V>(s.x + w * f.x, s.y + w * f.y);
+__device__ __forceinline__ double2 acc_add(double2 s, V f, decltype(V::x) w, decltype(V::x) wl) {
+  const double ww = static_cast<double>(w) + static_cast<double>(wl);
+  return make_double2(fma(ww, static_cast<double>(f.x), s.x), fma(ww, static_cast<double>(f.y), s.y));
+}
+template <typename V>
+__device__ __forceinline__ V acc_out(double2 s) {
+  return cmake<V>(static_cast<decltype(V::x)>(s.x), static_cast<decltype(V::x)>(s.y));
 }
 
 // x * exp(i A) from the exp(i A) table. The mixed form holds g = exp(i A) - 1 (FP32; applied as x + x g, see
@@ -249,7 +289,7 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
         w = cconj(w);
         wl = cconj(wl);
       }
-      v[t] = (n & (n - 1)) != 0 ? cmul_dd(v[t], w, wl) : cmul2(v[t], w, wl);  // see cmul_dd
+      v[t] = (n & (n - 1)) != 0 ? cmul_comp(v[t], w, wl) : cmul2(v[t], w, wl);  // see cmul_comp
     }
     small_dft<V, R>(v, tw, n, sign);
     const int o = (j / ns) * span + k;
@@ -518,14 +558,14 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
       int blk = -1;
       if (p <= a.mj_max) blk = a.mj_max + p;
       else if (p >= nphi - a.mj_max) blk = a.mj_max + (p - nphi);
-      V s = cmake<V>(0, 0);
+      Acc<V> s = acc_zero();
       if (blk >= 0) {
         const int nj = a.block_size[blk];
         const long long r0 = a.block_offset[blk] + t * nj;
         const V* f = fbr + c * n_rot + a.block_first[blk];
-        for (int j = 0; j < nj; ++j) s = cadd_scaled(s, f[j], leg[r0 + j], lo_real(leg, n_leg, r0 + j));
+        for (int j = 0; j < nj; ++j) s = acc_add(s, f[j], leg[r0 + j], lo_real(leg, n_leg, r0 + j));
       }
-      dvr0[c * dvr_col + t * ld + p] = s;
+      dvr0[c * dvr_col + t * ld + p] = acc_out<V>(s);
     }
     __syncthreads();
     V* cur = smem_fft(dvr0, dvr1, twp, a.pphi, +1, ncol * nt, 1, ld, 1);
@@ -551,10 +591,10 @@ __global__ void __launch_bounds__(256) potential_kernel(PotArgs<T> a) {
       const int jj = irot - a.block_first[blk];
       const int slot = a.block_slot[blk];
       const long long c0l = a.block_offset[blk] + jj;
-      V s = cmake<V>(0, 0);
+      Acc<V> sa = acc_zero();
       for (int t = 0; t < nt; ++t)
-        s = cadd_scaled(s, cur[c * dvr_col + t * ld + slot], leg[c0l + t * nj], lo_real(leg, n_leg, c0l + t * nj));
-      s = fmul_t(s, a.rot_half, n_scale, ir * n_rot + irot);
+        sa = acc_add(sa, cur[c * dvr_col + t * ld + slot], leg[c0l + t * nj], lo_real(leg, n_leg, c0l + t * nj));
+      const V s = fmul_t(acc_out<V>(sa), a.rot_half, n_scale, ir * n_rot + irot);
       const int ixy = c0 + c;
       if (irot == i0) i0buf[ixy] = s;
       else a.psi[(col_base + ixy) * n_rot + irot] = s;

@@ -194,10 +194,14 @@ namespace spo {
 // both levels: TB x N1 threads; thread (b, s) takes the first-level lines n2 = s and s + N1 of lane b
 // (two DFT_N1) and the second-level line k1 = s (one DFT_N2). In axis2_kernel (TB x N2 threads) half of
 // the threads wait at the barrier during the second level. Dynamic shared memory as axis2_kernel.
-// Mixed form: registers capped for eight blocks of 128 threads per SM (the pass waits on its global
-// loads; 64 registers with a 64-byte spill take Z = 128 from 1.38 to 1.29 ms on configuration 3).
+// Mixed form: registers capped for SPO_AXIS2B_SM_THREADS resident threads per SM (default 1024: eight
+// blocks of 128 threads; the pass waits on its global loads, and 64 registers with a 64-byte spill took
+// Z = 128 from 1.38 to 1.29 ms on configuration 3).
+#ifndef SPO_AXIS2B_SM_THREADS
+#define SPO_AXIS2B_SM_THREADS 1024
+#endif
 template <typename T, int N1, int N2, int TB>
-__global__ void __launch_bounds__(TB * N1, sizeof(T) == 4 ? 1024 / (TB * N1) : 1) axis2b_kernel(Axis2Args<T> a) {
+__global__ void __launch_bounds__(TB * N1, sizeof(T) == 4 ? SPO_AXIS2B_SM_THREADS / (TB * N1) : 1) axis2b_kernel(Axis2Args<T> a) {
   using V = Vec<T>;
   static_assert(N2 == 2 * N1, "the balanced form needs N2 = 2 N1");
   constexpr int N = N1 * N2;

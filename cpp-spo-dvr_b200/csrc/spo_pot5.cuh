@@ -102,21 +102,22 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
 // values), E (NT CB rows of NPHI + 2 values), X (NPHI padded slot blocks), the scaling rows with their
 // low parts (one opt_r rot(dt/2) row, two rot(dt/2) rows, CB incoming amplitudes), the matrix rows (n_rot rows of NT + 4),
 // irot -> slot (n_rot ints), the slot sizes and first rows (2 NPHI ints), the schedule (8 sched_len ints).
-// The L2E form keeps neither E nor the opt_r rot(dt/2) row in shared memory.
+// The L2E form keeps neither E nor the scaling rows in shared memory.
 template <typename T>
 constexpr std::size_t pot5_smem(int n_rot, int nphi, int nt, int cb, int sched_len, bool l2e = false) {
   return 32 + sizeof(Vec<T>) * (static_cast<std::size_t>(cb) * (n_rot + 2) +
                                 (l2e ? 0 : static_cast<std::size_t>(nt) * cb * (nphi + 2)) +
                                 static_cast<std::size_t>(nphi) * pot4_slot_stride<T>(nt, cb) +
-                                (l2e ? 4 : 6) * static_cast<std::size_t>(n_rot) + cb) +
+                                (l2e ? 0 : 6) * static_cast<std::size_t>(n_rot) + cb) +
          sizeof(T) * static_cast<std::size_t>(n_rot) * (nt + 4) +
          sizeof(int) * (static_cast<std::size_t>(n_rot) + 2 * nphi + 8 * sched_len);
 }
 
 // L2E: the exp(i A) rows are not staged in shared memory; each item's block of them is prefetched into
 // L2 one item ahead (cp.async.bulk.prefetch.L2) and every thread reads its row from there at the start of
-// its phi phase, and the opt_r rot(dt/2) values of a thread's rotational states come one item ahead into
-// registers. That leaves ~75 KB of shared memory per block: three blocks (12 warps) per SM instead of two.
+// its phi phase; the opt_r rot(dt/2) values of a thread's rotational states come one item ahead into
+// registers, and its rot(dt/2) values (with their low parts) are read through L1 at the start of the back
+// sums. That leaves ~72 KB of shared memory per block: three blocks (12 warps) per SM instead of two.
 template <typename T, int NPHI, int NT, int CB, bool L2E = false>
 __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Args<T> g, int* __restrict__ error_flag) {
   using V = Vec<T>;
@@ -139,8 +140,8 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
   V* X = E + (L2E ? 0 : NTH * ERS);        // [p][theta][c], slot blocks of SS values
   // The scaling rows hold each value and its low part (see cmul2): rows of n_rot values, then n_rot low parts.
   V* Bf = X + NPHI * SS;                   // [irot]: opt_r rot(dt/2) at the item's r point (not with L2E)
-  V* R = Bf + (L2E ? 0 : 2 * n_rot);       // [item parity][irot]: rot(dt/2) at the item's r point
-  V* SP = R + 4 * n_rot;                   // [c]: sp2sc(c) * chi, the item's incoming amplitudes
+  V* R = Bf + (L2E ? 0 : 2 * n_rot);       // [item parity][irot]: rot(dt/2) at the item's r point (not with L2E)
+  V* SP = R + (L2E ? 0 : 4 * n_rot);       // [c]: sp2sc(c) * chi, the item's incoming amplitudes
   T* L = reinterpret_cast<T*>(SP + CB);    // [irot][position of theta], rows of LDL
   int* irot_slot = reinterpret_cast<int*>(L + n_rot * LDL);
   int* s_nj = irot_slot + n_rot;           // [slot]: J count
@@ -185,8 +186,8 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     ncol = min(CB, a.n_xy - c0);
   };
   // Every thread arrives on each barrier once per phase; the threads that copy announce their bytes.
-  // Threads c < ncol copy column c; thread CB the opt_r rot(dt/2) row, thread CB + 1 the rot(dt/2) row
-  // (into R[parity]), CB + 2 its low parts, CB + 3 those of the opt_r rot(dt/2) row.
+  // Threads c < ncol copy column c; in the staged form thread CB the opt_r rot(dt/2) row, thread CB + 1 the
+  // rot(dt/2) row (into R[parity]), CB + 2 its low parts, CB + 3 those of the opt_r rot(dt/2) row.
   auto issue_psi = [&](long long item, int parity_r) {
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       pot5::mbar_arrive_tx(bars, col_bytes + (tid == 0 ? g.extra_tx : 0u));
       pot5::bulk_copy(F + tid * FCS, a.psi + (static_cast<long long>(izr) * a.n_xy + c0 + tid) * n_rot, col_bytes,
                       bars);
-    } else if (((tid == CB || tid == CB + 3) && !L2E) || tid == CB + 1 || tid == CB + 2) {
+    } else if (!L2E && tid >= CB && tid <= CB + 3) {
       pot5::fence_proxy_async();
       pot5::mbar_arrive_tx(bars, col_bytes);
       const long long row = static_cast<long long>(ir) * n_rot;
@@ -277,8 +278,10 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     int izr, c0, ncol;
     item_columns(item, izr, c0, ncol);
     const long long col_base = static_cast<long long>(izr) * a.n_xy + c0;
-    const V* rh_row = R + rp * 2 * n_rot;  // then its n_rot low parts
     const int ir_item = izr % a.nr;
+    // rot(dt/2) at the item's r point, then its n_rot low parts
+    const V* rh_row = L2E ? a.rot_half + static_cast<long long>(ir_item) * n_rot : R + rp * 2 * n_rot;
+    const long long rh_lo = L2E ? n_scale : n_rot;
     if (tid < CB) SP[tid] = cmul2(chi_in, sp_in, sp_lo);  // the previous item's scaling phase has read SP
 
     // ---- wait for the columns and rows, scale the columns in place (absorbers, rot(dt/2), the
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     // Two rotational states per pass, all their loads before the first store (the compiler cannot tell
     // that the runtime-strided stores to F miss the later loads, and would otherwise serialise them).
     {
-      const V rot_i0 = rh_row[i0], rot_i0_lo = rh_row[n_rot + i0];
+      const V rot_i0 = rh_row[i0], rot_i0_lo = rh_row[rh_lo + i0];
       const V sbi = sb;
       for (int ia = tid; ia < n_rot; ia += 2 * NTH) {
         const int ib = ia + NTH;
@@ -467,6 +470,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       const int ib = ia + NTH;
       const bool has_b = ib < n_rot;
       const int ibb = has_b ? ib : ia;
+      const V rh[2] = {rh_row[ia], rh_row[ibb]}, rhl[2] = {rh_row[rh_lo + ia], rh_row[rh_lo + ibb]};
       T acc[2][CB][2];
 #pragma unroll
       for (int u = 0; u < 2; ++u)
@@ -499,10 +503,9 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       for (int u = 0; u < 2; ++u) {
         const int irot = u == 0 ? ia : ib;
         if (u == 1 && !has_b) break;
-        const V rh = rh_row[irot], rhl = rh_row[n_rot + irot];
 #pragma unroll
         for (int c = 0; c < CB; ++c)
-          if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = fmul_parts(cmake<V>(acc[u][c][0], acc[u][c][1]), rh, rhl, one);
+          if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = fmul_parts(cmake<V>(acc[u][c][0], acc[u][c][1]), rh[u], rhl[u], one);
       }
     }
   }

@@ -94,26 +94,21 @@ SPO_HD V twiddle_mul(V a) {
     using R = decltype(V::x);
     constexpr R c = static_cast<R>(Root<k, N, S>::re);
     constexpr R s = static_cast<R>(Root<k, N, S>::im);
-    if constexpr (sizeof(R) == 4 && (N & (N - 1)) != 0) {
-      // mixed form, roots of lengths with an odd factor: the product in FP64, rounded once (with FP32
-      // partial sums these roots drift the norm of a pass by ~2e-9, the same sign every pass)
-      constexpr double cd = Root<k, N, S>::re, sd = Root<k, N, S>::im;
-      const double ax = a.x, ay = a.y;
-      return cmake<V>(static_cast<R>(ax * cd - ay * sd), static_cast<R>(ax * sd + ay * cd));
-    } else if constexpr (sizeof(R) == 4) {  // mixed form: the root as c + cl, s + sl (see cmul2)
+    if constexpr (sizeof(R) == 4) {  // mixed form: the root as c + cl, s + sl (see cmul2, cmul_comp)
       constexpr R cl = static_cast<R>(Root<k, N, S>::re - static_cast<double>(c));
       constexpr R sl = static_cast<R>(Root<k, N, S>::im - static_cast<double>(s));
-      return cmul2(a, cmake<V>(c, s), cmake<V>(cl, sl));
+      if constexpr ((N & (N - 1)) != 0) return cmul_comp(a, cmake<V>(c, s), cmake<V>(cl, sl));
+      else return cmul2(a, cmake<V>(c, s), cmake<V>(cl, sl));
     } else {
       return cmake<V>(a.x * c - a.y * s, a.x * s + a.y * c);
     }
   }
 }
 
-// A runtime twiddle of a length-N transform: FP64 product for lengths with an odd factor, else cmul2.
+// A runtime twiddle of a length-N transform: cmul_comp for lengths with an odd factor, else cmul2.
 template <int N, typename V>
 SPO_HD V tw_mul(V a, V w, V wl) {
-  if constexpr ((N & (N - 1)) != 0) return cmul_dd(a, w, wl);
+  if constexpr ((N & (N - 1)) != 0) return cmul_comp(a, w, wl);
   else return cmul2(a, w, wl);
 }
 
@@ -151,12 +146,14 @@ SPO_HD void rdft(V (&x)[N]) {
     x[3] = csub(d02, jd);
   } else if constexpr (N == 3 || N == 5 || N == 7 || N == 11) {
     // Odd prime: pairs (t, N - t) share the real part of the root and have opposite imaginary parts.
-    // The mixed form sums each output pair in FP64 from the FP32 sums and differences and rounds once: summed
-    // in FP32, the shared partial sums of the pair drift the norm of a forward-inverse pass with a phase
-    // between them by ~2e-8 (radix 3), the same sign every pass.
+    // Mixed form: radix 3 (one term per output pair) holds its root as two FP32 values (see cmul2) and adds
+    // the small part's product first; radices 5, 7 and 11 sum each output pair in FP64 from the FP32 sums and
+    // differences and round once. With the roots rounded to FP32, a forward-inverse pass with a phase
+    // between them drifts the norm by ~2e-8 (radix 3); with exact roots but partial sums rounded in FP32,
+    // by ~7e-9 (radix 5) and ~1e-8 (radix 7), the same sign every pass.
     using R = decltype(V::x);
-    using A = std::conditional_t<sizeof(R) == 4, double, R>;  // accumulation type
     constexpr int H = N / 2;
+    using A = std::conditional_t<sizeof(R) == 4 && H >= 2, double, R>;  // accumulation type
     V s[H + 1], d[H + 1];
     static_for<1, H + 1>([&](auto t) {
       s[t] = cadd(x[t], x[N - t]);
@@ -172,10 +169,19 @@ SPO_HD void rdft(V (&x)[N]) {
         constexpr long tq = static_cast<long>(SPO_CV(t)) * SPO_CV(q) % N;
         constexpr A c = static_cast<A>(Root<tq, N, S>::re);
         constexpr A sn = static_cast<A>(Root<tq, N, S>::im);
-        rex += c * static_cast<A>(s[t].x);
-        rey += c * static_cast<A>(s[t].y);
-        ir += sn * static_cast<A>(d[t].x);
-        ii += sn * static_cast<A>(d[t].y);
+        if constexpr (sizeof(A) == 4) {  // mixed form, radix 3
+          constexpr A cl = static_cast<A>(Root<tq, N, S>::re - static_cast<double>(c));
+          constexpr A sl = static_cast<A>(Root<tq, N, S>::im - static_cast<double>(sn));
+          rex = fmaf(c, s[t].x, fmaf(cl, s[t].x, rex));
+          rey = fmaf(c, s[t].y, fmaf(cl, s[t].y, rey));
+          ir = fmaf(sn, d[t].x, fmaf(sl, d[t].x, ir));
+          ii = fmaf(sn, d[t].y, fmaf(sl, d[t].y, ii));
+        } else {
+          rex += c * static_cast<A>(s[t].x);
+          rey += c * static_cast<A>(s[t].y);
+          ir += sn * static_cast<A>(d[t].x);
+          ii += sn * static_cast<A>(d[t].y);
+        }
       });
       out[q] = cmake<V>(static_cast<R>(rex - ii), static_cast<R>(rey + ir));  // re + i * sum Im(w) d
       out[N - q] = cmake<V>(static_cast<R>(rex + ii), static_cast<R>(rey - ir));
@@ -235,10 +241,14 @@ struct Axis2Args {
 };
 
 // Dynamic shared memory: (N TB + 2 N) values (axis2_smem).
-// Mixed form with at most 8 sub-rows: registers capped for 1536 threads per SM (r = 48 = 6 x 8 at 40
-// registers: six blocks of 256 threads instead of five, 1.23 -> 1.12 ms on configuration 3).
+// Mixed form with at most 8 sub-rows: registers capped for SPO_AXIS2_SM_THREADS resident threads per SM
+// (default 1536: r = 48 = 6 x 8 at 40 registers, six blocks of 256 threads instead of five, took 1.23 ->
+// 1.12 ms on configuration 3).
+#ifndef SPO_AXIS2_SM_THREADS
+#define SPO_AXIS2_SM_THREADS 1536
+#endif
 template <typename T, int N1, int N2, int TB>
-__global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2), sizeof(T) == 4 && (N1 > N2 ? N1 : N2) <= 8 ? 1536 / (TB*(N1 > N2 ? N1 : N2)) : 1) axis2_kernel(Axis2Args<T> a) {
+__global__ void __launch_bounds__(TB*(N1 > N2 ? N1 : N2), sizeof(T) == 4 && (N1 > N2 ? N1 : N2) <= 8 ? SPO_AXIS2_SM_THREADS / (TB*(N1 > N2 ? N1 : N2)) : 1) axis2_kernel(Axis2Args<T> a) {
   using V = Vec<T>;
   constexpr int N = N1 * N2;
   constexpr int NS = N1 > N2 ? N1 : N2;
@@ -448,7 +458,7 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
       static_for<0, NPHI>([&](auto p) {
         constexpr int P = SPO_CV(p);
         const int m = P <= mj_max ? P : (P >= NPHI - mj_max ? P - NPHI : 1 << 20);
-        V s = cmake<V>(0, 0);
+        Acc<V> s = acc_zero();
         if (m != (1 << 20)) {
           const int blk = mj_max + m;
           const int nj = a.block_size[blk];
@@ -456,10 +466,10 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
           const long long m0 = a.block_offset[blk] + t;  // (J, theta) within the block
           for (int j = 0; j < nj; ++j) {
             const long long k = m0 + j * nt;
-            s = cadd_scaled(s, f[first + j], __ldg(args.legendre_t + k), lo_real(args.legendre_t, n_leg, k));
+            s = acc_add(s, f[first + j], __ldg(args.legendre_t + k), lo_real(args.legendre_t, n_leg, k));
           }
         }
-        x[P] = s;
+        x[P] = acc_out<V>(s);
       });
       rdft<NPHI, +1>(x);
       if (args.identity_maps) {
@@ -483,19 +493,19 @@ __global__ void __launch_bounds__(128) potential2_kernel(Pot2Args<T> args) {
       const int jj = irot - a.block_first[blk];
       const int slot = a.block_slot[blk];
       const long long c0l = a.block_offset[blk] + jj;
-      V acc[CB];
+      Acc<V> acc[CB];
 #pragma unroll
-      for (int c = 0; c < CB; ++c) acc[c] = cmake<V>(0, 0);
+      for (int c = 0; c < CB; ++c) acc[c] = acc_zero();
       for (int t = 0; t < nt; ++t) {
         const T w = leg[c0l + t * nj], wl = lo_real(leg, n_leg, c0l + t * nj);
         const V* d = D + t * LD + slot;
 #pragma unroll
-        for (int c = 0; c < CB; ++c) acc[c] = cadd_scaled(acc[c], d[c * nt * LD], w, wl);
+        for (int c = 0; c < CB; ++c) acc[c] = acc_add(acc[c], d[c * nt * LD], w, wl);
       }
 #pragma unroll
       for (int c = 0; c < CB; ++c) {
         if (c < ncol) {
-          const V s = fmul_t(acc[c], a.rot_half, n_scale, ir * n_rot + irot);
+          const V s = fmul_t(acc_out<V>(acc[c]), a.rot_half, n_scale, ir * n_rot + irot);
           if (irot == i0) i0buf[c0 + c] = s;
           else a.psi[(col_base + c0 + c) * n_rot + irot] = s;
         }
@@ -587,14 +597,16 @@ __global__ void __launch_bounds__(CB * 16) potential3_kernel(Pot2Args<T> args) {
     const V* f = F + line_c * FS;
     const T* mt = args.legendre_slot + line_t;
     const long long n_slot = static_cast<long long>(NPHI) * jp * nt;  // low parts follow (mixed form)
-    static_for<0, NPHI>([&](auto p) { x[p] = cmake<V>(0, 0); });
+    Acc<V> xa[NPHI];
+    static_for<0, NPHI>([&](auto p) { xa[p] = acc_zero(); });
     for (int j = 0; j < jp; ++j) {
       static_for<0, NPHI>([&](auto p) {
         constexpr int P = SPO_CV(p);
         const long long k = (P * jp + j) * nt;
-        x[P] = cadd_scaled(x[P], f[P * jp + j], __ldg(mt + k), lo_real(mt, n_slot, k));
+        xa[P] = acc_add(xa[P], f[P * jp + j], __ldg(mt + k), lo_real(mt, n_slot, k));
       });
     }
+    static_for<0, NPHI>([&](auto p) { x[p] = acc_out<V>(xa[p]); });
   }
   __syncthreads();  // F is consumed; D takes its memory
   if (has_line) {
@@ -622,19 +634,19 @@ __global__ void __launch_bounds__(CB * 16) potential3_kernel(Pot2Args<T> args) {
     const int slot = __ldg(a.block_slot + blk);
     const T* col = a.legendre + __ldg(a.block_offset + blk) + jj;  // (theta, J) within the block
     const long long n_leg = static_cast<long long>(nt) * n_rot;      // low parts follow (mixed form)
-    V acc[CB];
+    Acc<V> acc[CB];
 #pragma unroll
-    for (int c = 0; c < CB; ++c) acc[c] = cmake<V>(0, 0);
+    for (int c = 0; c < CB; ++c) acc[c] = acc_zero();
     for (int t = 0; t < nt; ++t) {
       const T w = __ldg(col + t * nj), wl = lo_real(col, n_leg, t * nj);
       const V* d = D + t * LD + slot;
 #pragma unroll
-      for (int c = 0; c < CB; ++c) acc[c] = cadd_scaled(acc[c], d[c * nt * LD], w, wl);
+      for (int c = 0; c < CB; ++c) acc[c] = acc_add(acc[c], d[c * nt * LD], w, wl);
     }
     const long long n_scale = static_cast<long long>(a.nr) * n_rot;
 #pragma unroll
     for (int c = 0; c < CB; ++c)
-      if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = fmul_t(acc[c], a.rot_half, n_scale, ir * n_rot + irot);
+      if (c < ncol) a.psi[(col_base + c) * n_rot + irot] = fmul_t(acc_out<V>(acc[c]), a.rot_half, n_scale, ir * n_rot + irot);
   }
 }
 
