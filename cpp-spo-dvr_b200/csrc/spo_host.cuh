@@ -231,8 +231,62 @@ bool launch_axis2_n(const spo::Axis2Args<T>& a, long long outer, cudaStream_t st
   }
 }
 
+// The prime-factor splits N = N1 x N2 (N1, N2 coprime) with an axis2pfa_kernel instantiation; LT threads per
+// batch lane (LT >= N1).
+inline bool pfa_split(int n, int& n1, int& n2) {
+  switch (n) {
+    case 24: n1 = 3; n2 = 8; return true;
+    case 40: n1 = 5; n2 = 8; return true;
+    case 48: n1 = 3; n2 = 16; return true;
+    case 56: n1 = 7; n2 = 8; return true;
+    case 80: n1 = 5; n2 = 16; return true;
+    case 112: n1 = 7; n2 = 16; return true;
+    default: return false;
+  }
+}
+// Position k1 + N1 k2 of the prime-factor order holds the factor of momentum index
+// k = (N2 u k1 + N1 v k2) mod N, u = N2^-1 mod N1, v = N1^-1 mod N2 (axis2pfa_kernel).
+template <typename C>
+std::vector<C> pfa_order(const std::vector<C>& f, int n1, int n2) {
+  const int n = n1 * n2, u = spo::pfa_inverse(n2 % n1, n1), v = spo::pfa_inverse(n1 % n2, n2);
+  std::vector<C> out(f.size());
+  for (int k1 = 0; k1 < n1; ++k1)
+    for (int k2 = 0; k2 < n2; ++k2) out[k1 + n1 * k2] = f[(static_cast<long long>(n2) * u * k1 + static_cast<long long>(n1) * v * k2) % n];
+  return out;
+}
+template <typename T, int N1, int N2, int LT>
+bool launch_axis2_pfa_n(const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
+  constexpr int TB = 32, N = N1 * N2;
+  const std::size_t smem = sizeof(spo::Vec<T>) * (static_cast<std::size_t>(N) * TB + (sizeof(T) == 4 ? spo::kFactorParts : 1) * N);
+  static unsigned long long configured = 0;
+  allow_smem(spo::axis2pfa_kernel<T, N1, N2, TB, LT>, smem, configured, "axis2pfa smem");
+  spo::Axis2Args<T> w = a;
+  unsigned blocks_x;
+  if (a.window > 0) {
+    w.blocks_per_group = static_cast<int>((a.window + TB - 1) / TB);
+    blocks_x = static_cast<unsigned>(a.groups * w.blocks_per_group);
+  } else {
+    blocks_x = static_cast<unsigned>((a.inner + TB - 1) / TB);
+  }
+  spo::axis2pfa_kernel<T, N1, N2, TB, LT><<<dim3(blocks_x, static_cast<unsigned>(outer)), TB * LT, smem, stream>>>(w);
+  return true;
+}
+template <typename T>
+bool launch_axis2_pfa(int n, const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
+  switch (n) {
+    case 24: return launch_axis2_pfa_n<T, 3, 8, 4>(a, outer, stream);
+    case 40: return launch_axis2_pfa_n<T, 5, 8, 8>(a, outer, stream);
+    case 48: return launch_axis2_pfa_n<T, 3, 16, 4>(a, outer, stream);
+    case 56: return launch_axis2_pfa_n<T, 7, 8, 8>(a, outer, stream);
+    case 80: return launch_axis2_pfa_n<T, 5, 16, 8>(a, outer, stream);
+    case 112: return launch_axis2_pfa_n<T, 7, 16, 8>(a, outer, stream);
+    default: return false;
+  }
+}
+
 template <typename T>
 bool launch_axis2(int n, const spo::Axis2Args<T>& a, long long outer, cudaStream_t stream) {
+  if (a.factor_pfa && !a.persistent) return launch_axis2_pfa<T>(n, a, outer, stream);
   switch (n) {
     // N = N1 N2 with N2 >= N1: the first level, which streams the tile in from HBM, uses every thread.
     case 24: return launch_axis2_n<T, 4, 6>(a, outer, stream);
@@ -518,11 +572,23 @@ class Profiler {
   std::size_t used_ = 0;
 };
 
+// v rounded to `bits` significant bits (nearest).
+inline double round_bits(double v, int bits) {
+  if (v == 0.0 || !std::isfinite(v)) return v;
+  int e = 0;
+  std::frexp(v, &e);
+  const double q = std::ldexp(1.0, e - bits);
+  return std::nearbyint(v / q) * q;
+}
+
 // Rounds a matrix to FP32 row by row so that each row's sum of squares is as close to its FP64 value as
 // the roundings allow: every entry takes one of its two FP32 neighbours, chosen by a meet-in-the-middle
 // search over the entries' alternatives (rows of up to 24 non-zero entries; longer rows keep the nearest
-// rounding). A matrix applied with its transpose at every time step (the theta contractions) then changes
-// the norm of a state only by the unbiased rounding of the arithmetic, not by its entries' rounding.
+// rounding). A matrix applied with its transpose at every time step (the theta contractions) then keeps the
+// norm of a random state (whose rotational components have independent phases); on a physical wave packet
+// the other entries of the Gram matrix still act, which is why potential5 and the small-grid kernels use
+// the matrix to ~2^-36 (12-bit high parts with their remainders, or FP64 sums) and only potential4's mixed
+// form uses these FP32 rows alone.
 inline std::vector<float> norm_preserving_rows(const std::vector<double>& m, int rows, int stride) {
   std::vector<float> out(m.size());
   for (std::size_t i = 0; i < m.size(); ++i) out[i] = static_cast<float>(m[i]);
@@ -664,6 +730,9 @@ class Step final : public StepBase {
     auto lanes = [](int tile, bool has_tiles) { return "tb" + std::to_string(!has_tiles ? 32 : tile ? tile : 16); };
     auto axis_name = [&](int n, int tile, bool persistent) {
       if (!(use_v2_ && axis2_supported(n))) return std::string("axis_pass(general)");
+      int n1 = 0, n2 = 0;
+      if (use_pfa_ && !persistent && pfa_split(n, n1, n2))
+        return "axis2pfa<" + std::to_string(n) + "=" + std::to_string(n1) + "x" + std::to_string(n2) + ",tb32>";
       const char* form = zr_window_ > 0 ? "axis2" : persistent ? "axis2p" : balanced_ && axis2_balanced(n) ? "axis2b" : "axis2";
       return form + std::string("<") + std::to_string(n) + "," + lanes(tile, axis2_has_tiles(n)) + ">";
     };
@@ -982,6 +1051,7 @@ class Step final : public StepBase {
     for (int iz0 = 0; iz0 < s_.nz; iz0 += rxy_planes_) {
       const int g = std::min(rxy_planes_, s_.nz - iz0);
       spo::Axis2Args<T> r{psi_ + plane * iz0, s_.n_xy() * s_.n_rot, half ? rk_half_ : rk_full_, tw_r_, tile_r_};
+      r.factor_pfa = pfa_of(r.factor);
       r.persistent = persist_r_ ? 1 : 0;
       prof_.begin(stream_);
       launch_axis2<T>(plan_r_.n, r, g, stream_);
@@ -1019,6 +1089,7 @@ class Step final : public StepBase {
       const long long w = std::min<long long>(zr_window_, lanes - l0);
       const double bw = b * static_cast<double>(w) / static_cast<double>(lanes);
       spo::Axis2Args<T> z{psi_, 0, zf, tw_z_, tile_z_};
+      z.factor_pfa = pfa_of(zf);
       z.groups = s_.nr;  // lanes (ir, l0 + l): groups ir, lanes apart
       z.group_stride = lanes;
       z.lane_offset = l0;
@@ -1030,6 +1101,7 @@ class Step final : public StepBase {
       prof_.end(stream_, "kinetic_z", bw);
       ++launches_;
       spo::Axis2Args<T> r{psi_, 0, rf, tw_r_, tile_r_};
+      r.factor_pfa = pfa_of(rf);
       r.groups = 1;
       r.group_stride = 0;
       r.lane_offset = l0;
@@ -1045,10 +1117,20 @@ class Step final : public StepBase {
 
   // A kinetic axis pass over psi: the register-DFT kernel for its length when instantiated, else the
   // general Stockham kernel.
+  // The prime-factor-order copy of a Z or r factor table (null when that axis has no prime-factor split).
+  const V* pfa_of(const V* factor) const {
+    if (!use_pfa_ || !use_v2_) return nullptr;
+    if (factor == zk_full_) return zk_full_pfa_;
+    if (factor == zk_half_) return zk_half_pfa_;
+    if (factor == rk_full_) return rk_full_pfa_;
+    if (factor == rk_half_) return rk_half_pfa_;
+    return nullptr;
+  }
   void axis_psi(const char* name, double bytes, long long outer, const spo::FftPlan& plan, const V* tw,
                 long long inner, const V* factor, int tile, bool persistent = false, bool balanced = false) {
     if (use_v2_ && axis2_supported(plan.n)) {
       spo::Axis2Args<T> a{psi_, inner, factor, tw, tile};
+      a.factor_pfa = pfa_of(factor);
       a.persistent = persistent ? 1 : 0;
       a.balanced = balanced ? 1 : 0;
       prof_.begin(stream_);
@@ -1435,6 +1517,17 @@ class Step final : public StepBase {
     zk_half_ = upload_factor(scaled(complex_array(d.z_kinetic_half, s.nz, "z_kinetic_half"), 1.0 / s.nz));
     rk_full_ = upload_factor(scaled(complex_array(d.r_kinetic_full, s.nr, "r_kinetic_full"), 1.0 / s.nr));
     rk_half_ = upload_factor(scaled(complex_array(d.r_kinetic_half, s.nr, "r_kinetic_half"), 1.0 / s.nr));
+    {  // the same factors in the prime-factor order (axis2pfa_kernel), for axes with such a split
+      int n1 = 0, n2 = 0;
+      if (pfa_split(s.nz, n1, n2)) {
+        zk_full_pfa_ = upload_factor(pfa_order(scaled(complex_array(d.z_kinetic_full, s.nz, "z_kinetic_full"), 1.0 / s.nz), n1, n2));
+        zk_half_pfa_ = upload_factor(pfa_order(scaled(complex_array(d.z_kinetic_half, s.nz, "z_kinetic_half"), 1.0 / s.nz), n1, n2));
+      }
+      if (pfa_split(s.nr, n1, n2)) {
+        rk_full_pfa_ = upload_factor(pfa_order(scaled(complex_array(d.r_kinetic_full, s.nr, "r_kinetic_full"), 1.0 / s.nr), n1, n2));
+        rk_half_pfa_ = upload_factor(pfa_order(scaled(complex_array(d.r_kinetic_half, s.nr, "r_kinetic_half"), 1.0 / s.nr), n1, n2));
+      }
+    }
     const double sx = s.nx > 1 ? d.fft_scale_x : 1.0;
     const double sy = s.ny > 1 ? d.fft_scale_y : 1.0;
     const double xy_scale = (sx * sy) * ((1.0 / (s.nx * sx)) * (1.0 / (s.ny * sy)));
@@ -1748,7 +1841,7 @@ class Step final : public StepBase {
           sched[(2 * w) * len + k] = warp[w][k].a;
           sched[(2 * w + 1) * len + k] = warp[w][k].b;
         }
-      std::vector<double> rows(static_cast<std::size_t>(s.n_rot) * (nt_k + 4), 0.0);
+      std::vector<double> rows(static_cast<std::size_t>(s.n_rot) * (nt_k + 4), 0.0), rows12(rows), rows_lo(rows);
       std::vector<int> irot_slot(s.n_rot);
       for (int b = 0; b < s.n_blocks; ++b)
         for (int j = 0; j < size[b]; ++j) {
@@ -1756,11 +1849,17 @@ class Step final : public StepBase {
           for (int t = 0; t < s.nt; ++t) {  // theta t >= s.nt (padding) stays zero
             const int quads = nt_k / 4;  // theta t at the position where the forward tiles read it
             const int pos = (t % quads) * 4 + t / quads;
-            rows[static_cast<std::size_t>(first[b] + j) * (nt_k + 4) + pos] = legendre[offset[b] + t * size[b] + j];
+            const std::size_t k = static_cast<std::size_t>(first[b] + j) * (nt_k + 4) + pos;
+            rows[k] = legendre[offset[b] + t * size[b] + j];
+            const double v = legendre64[offset[b] + t * size[b] + j];
+            rows12[k] = round_bits(v, 12);
+            rows_lo[k] = v - rows12[k];
           }
         }
       pot4_args_.p = pot2_.p;
       pot4_args_.leg_rows = upload_real(rows);
+      pot4_args_.leg_rows12 = sizeof(T) == 4 ? upload_real(rows12) : nullptr;
+      pot4_args_.leg_rows_lo = sizeof(T) == 4 ? upload_real(rows_lo) : nullptr;
       pot4_args_.slot_first = upload_int(slot_first);
       pot4_args_.slot_nj = upload_int(slot_nj);
       pot4_args_.irot_slot = upload_int(irot_slot);
@@ -1878,6 +1977,8 @@ class Step final : public StepBase {
     if (use_v2_ && pot4_kernel_) pot_kind_ = 4;
     if (use_v2_ && pot5_kernel_) pot_kind_ = 5;
     pot_source_ = "default";
+    use_pfa_ = true;
+    if (const char* env = std::getenv("SPO_B200_PFA")) use_pfa_ = std::string(env) != "0";
     if (const char* env = std::getenv("SPO_B200_KERNELS")) {
       const std::string k(env);
       require(k == "v1" || k == "v2" || k == "v3" || k == "v4" || k == "v5" || k == "v6",
@@ -1955,6 +2056,9 @@ class Step final : public StepBase {
   int pot2_cb_ = 0;
   std::size_t pot2_smem_ = 0;
   bool use_v2_ = true;  // register-DFT kernels where instantiated (SPO_B200_KERNELS=v1: the general kernels)
+  // Z and r lengths with a prime-factor split run axis2pfa_kernel (SPO_B200_PFA=0: the kernels with twiddles)
+  bool use_pfa_ = true;
+  V *zk_full_pfa_ = nullptr, *zk_half_pfa_ = nullptr, *rk_full_pfa_ = nullptr, *rk_half_pfa_ = nullptr;
   spo::Pot2Args<T> pot3_args_{};
   int pot3_cb_ = 0, pot3_chunks_ = 0;
   std::size_t pot3_smem_ = 0;

@@ -32,6 +32,11 @@ struct Pot4Args {
   PotArgs<T> p;              // pointers and sizes shared with the other potential kernels
   const T* leg_rows;         // n_rot rows of NT + 4: M_m[theta, J] of irot = first_m + J, theta at position
                              // (theta % (NT / 4)) * 4 + theta / (NT / 4)
+  // potential5 (mixed form): the same rows as a 12-bit high part and the FP32 rounding of the rest, so that
+  // hi + lo is the FP64 matrix to ~2^-36 and each term's lo product stays well above the rounding unit of
+  // the running sum (see potential5_kernel)
+  const T* leg_rows12;
+  const T* leg_rows_lo;
   const int* slot_first;     // per phi slot: first irot of its mJ block
   const int* slot_nj;        // per phi slot: J count (0: no basis functions)
   const int* irot_slot;      // per irot: its phi slot
@@ -113,12 +118,14 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
   V* X = F + n_rot * CB;                                   // [p][theta][c], slot blocks of SS values
   constexpr bool L_SHARED = pot4_matrix_shared<T>();
   T* Ls = reinterpret_cast<T*>(X + NPHI * SS);             // [irot][position of theta], rows of LDL
-  const T* L = L_SHARED ? Ls : g.leg_rows;
+  // the mixed form's matrix as 12-bit high parts plus the rest, as potential5 uses it
+  const T* rows = sizeof(T) == 4 ? g.leg_rows12 : g.leg_rows;
+  const T* L = L_SHARED ? Ls : rows;
   int* irot_slot = reinterpret_cast<int*>(Ls + (L_SHARED ? n_rot * LDL : 0));
   int* sched = irot_slot + n_rot;                          // [group][k]
   const int tid = threadIdx.x;
   if constexpr (L_SHARED)
-    for (int k = tid; k < n_rot * LDL; k += NTH) Ls[k] = g.leg_rows[k];
+    for (int k = tid; k < n_rot * LDL; k += NTH) Ls[k] = rows[k];
   for (int k = tid; k < n_rot; k += NTH) irot_slot[k] = g.irot_slot[k];
   for (int k = tid; k < 8 * g.sched_len; k += NTH) sched[k] = g.fwd_sched[k];
   __syncthreads();
@@ -212,12 +219,24 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
         ld4(lp + j * LDL, l);
         V f0, f1;
         ld2c(fp + j * CB, f0, f1);
+        if constexpr (sizeof(T) == 4) {
+          T m[4];
+          ld4(g.leg_rows_lo + (first + j) * LDL + 4 * fq, m);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          acc[q][0] += l[q] * f0.x;
-          acc[q][1] += l[q] * f0.y;
-          acc[q][2] += l[q] * f1.x;
-          acc[q][3] += l[q] * f1.y;
+          for (int q = 0; q < 4; ++q) {
+            acc[q][0] = fmaf(l[q], f0.x, fmaf(m[q], f0.x, acc[q][0]));
+            acc[q][1] = fmaf(l[q], f0.y, fmaf(m[q], f0.y, acc[q][1]));
+            acc[q][2] = fmaf(l[q], f1.x, fmaf(m[q], f1.x, acc[q][2]));
+            acc[q][3] = fmaf(l[q], f1.y, fmaf(m[q], f1.y, acc[q][3]));
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            acc[q][0] += l[q] * f0.x;
+            acc[q][1] += l[q] * f0.y;
+            acc[q][2] += l[q] * f1.x;
+            acc[q][3] += l[q] * f1.y;
+          }
         }
       }
 #pragma unroll
@@ -280,8 +299,9 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
       const V* ys = X + slot * SS;
 #pragma unroll 1
       for (int kq = 0; kq < QUADS; ++kq) {
-        T l[4];
+        T l[4], m[4] = {0, 0, 0, 0};
         ld4(lrow + 4 * kq, l);  // theta kq + QUADS q, q < 4
+        if constexpr (sizeof(T) == 4) ld4(g.leg_rows_lo + irot * LDL + 4 * kq, m);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const V* y = ys + (kq + QUADS * q) * CB;
@@ -289,10 +309,17 @@ __global__ void __launch_bounds__(NT * CB, sizeof(T) == 4 ? 3 : 1) potential4_ke
           for (int c = 0; c < CB; c += 2) {
             V y0, y1;
             ld2c(y + c, y0, y1);
-            acc[c][0] += l[q] * y0.x;
-            acc[c][1] += l[q] * y0.y;
-            acc[c + 1][0] += l[q] * y1.x;
-            acc[c + 1][1] += l[q] * y1.y;
+            if constexpr (sizeof(T) == 4) {
+              acc[c][0] = fmaf(l[q], y0.x, fmaf(m[q], y0.x, acc[c][0]));
+              acc[c][1] = fmaf(l[q], y0.y, fmaf(m[q], y0.y, acc[c][1]));
+              acc[c + 1][0] = fmaf(l[q], y1.x, fmaf(m[q], y1.x, acc[c + 1][0]));
+              acc[c + 1][1] = fmaf(l[q], y1.y, fmaf(m[q], y1.y, acc[c + 1][1]));
+            } else {
+              acc[c][0] += l[q] * y0.x;
+              acc[c][1] += l[q] * y0.y;
+              acc[c + 1][0] += l[q] * y1.x;
+              acc[c + 1][1] += l[q] * y1.y;
+            }
           }
         }
       }

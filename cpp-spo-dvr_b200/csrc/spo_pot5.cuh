@@ -113,6 +113,16 @@ constexpr std::size_t pot5_smem(int n_rot, int nphi, int nt, int cb, int sched_l
          sizeof(int) * (static_cast<std::size_t>(n_rot) + 2 * nphi + 8 * sched_len);
 }
 
+// The theta contractions use the matrix as a 12-bit high part (staged in shared memory) plus the FP32
+// rounding of the rest (read through L1), each term as fma(hi, x, fma(lo, x, acc)): hi + lo is the FP64
+// matrix to ~2^-36, and the lo products (~2^-13 of a term) stay well above the rounding unit of the sum, so
+// the sums round without bias. With the matrix rounded to FP32 alone (even with each rotational state's
+// sum of squares kept), the forward and transposed contractions of a physical wave packet (few rotational
+// states with turning relative phases, smooth in theta, the potential varying with theta) changed its norm
+// by up to ~1e-8 per step, the same sign every step: 5e-5 in P_reaction over 20000 steps of configuration 3.
+// With hi + lo as an FP32 value and its small remainder, the remainders lie below half an ulp of the
+// running sum and are rounded away.
+//
 // L2E: the exp(i A) rows are not staged in shared memory; each item's block of them is prefetched into
 // L2 one item ahead (cp.async.bulk.prefetch.L2) and every thread reads its row from there at the start of
 // its phi phase; the opt_r rot(dt/2) values of a thread's rotational states come one item ahead into
@@ -152,7 +162,7 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
     for (int k = 0; k < 2; ++k) pot5::mbar_init(bars + k, NTH);
     pot5::mbar_init_fence();
   }
-  for (int k = tid; k < n_rot * LDL; k += NTH) L[k] = g.leg_rows[k];
+  for (int k = tid; k < n_rot * LDL; k += NTH) L[k] = g.leg_rows12[k];
   for (int k = tid; k < n_rot; k += NTH) irot_slot[k] = g.irot_slot[k];
   for (int k = tid; k < NPHI; k += NTH) {
     s_nj[k] = g.slot_nj[k];
@@ -344,20 +354,22 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       for (int q = 0; q < 4; ++q)
 #pragma unroll
         for (int r = 0; r < 4; ++r) acc[q][r] = 0;
-      const T* lp = L + first * LDL + 4 * fq;
       const V* f0p = F + (2 * fc) * FCS + first;
       const V* f1p = f0p + FCS;
+      const T* lp = L + first * LDL + 4 * fq;                 // the entries' 12-bit high parts
+      const T* lq = g.leg_rows_lo + first * LDL + 4 * fq;     // and the rest (through L1)
       for (int j = 0; j < nj; ++j) {
-        T l[4];
+        T l[4], m[4];
         ld4(lp + j * LDL, l);
+        ld4(lq + j * LDL, m);
         const V f0 = f0p[j];
         const V f1 = f1p[j];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          acc[q][0] += l[q] * f0.x;
-          acc[q][1] += l[q] * f0.y;
-          acc[q][2] += l[q] * f1.x;
-          acc[q][3] += l[q] * f1.y;
+          acc[q][0] = fmaf(l[q], f0.x, fmaf(m[q], f0.x, acc[q][0]));
+          acc[q][1] = fmaf(l[q], f0.y, fmaf(m[q], f0.y, acc[q][1]));
+          acc[q][2] = fmaf(l[q], f1.x, fmaf(m[q], f1.x, acc[q][2]));
+          acc[q][3] = fmaf(l[q], f1.y, fmaf(m[q], f1.y, acc[q][3]));
         }
       }
 #pragma unroll
@@ -476,13 +488,16 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
       for (int u = 0; u < 2; ++u)
 #pragma unroll
         for (int c = 0; c < CB; ++c) acc[u][c][0] = acc[u][c][1] = 0;
-      const T* lrow[2] = {L + ia * LDL, L + ibb * LDL};
       const V* ys[2] = {X + irot_slot[ia] * SS, X + irot_slot[ibb] * SS};
+      const T* lrow[2] = {L + ia * LDL, L + ibb * LDL};                          // 12-bit high parts
+      const T* lrest[2] = {g.leg_rows_lo + ia * LDL, g.leg_rows_lo + ibb * LDL};  // the rest, through L1
 #pragma unroll 1
       for (int kq = 0; kq < QUADS; ++kq) {
-        T l[2][4];
+        T l[2][4], m[2][4];
         ld4(lrow[0] + 4 * kq, l[0]);
         ld4(lrow[1] + 4 * kq, l[1]);
+        ld4(lrest[0] + 4 * kq, m[0]);
+        ld4(lrest[1] + 4 * kq, m[1]);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
 #pragma unroll
@@ -491,10 +506,10 @@ __global__ void __launch_bounds__(NT * CB, L2E ? 3 : 2) potential5_kernel(Pot4Ar
             for (int u = 0; u < 2; ++u) {
               V y0, y1;
               ld2c(ys[u] + (kq + QUADS * q) * CB + c, y0, y1);
-              acc[u][c][0] += l[u][q] * y0.x;
-              acc[u][c][1] += l[u][q] * y0.y;
-              acc[u][c + 1][0] += l[u][q] * y1.x;
-              acc[u][c + 1][1] += l[u][q] * y1.y;
+              acc[u][c][0] = fmaf(l[u][q], y0.x, fmaf(m[u][q], y0.x, acc[u][c][0]));
+              acc[u][c][1] = fmaf(l[u][q], y0.y, fmaf(m[u][q], y0.y, acc[u][c][1]));
+              acc[u][c + 1][0] = fmaf(l[u][q], y1.x, fmaf(m[u][q], y1.x, acc[u][c + 1][0]));
+              acc[u][c + 1][1] = fmaf(l[u][q], y1.y, fmaf(m[u][q], y1.y, acc[u][c + 1][1]));
             }
           }
         }

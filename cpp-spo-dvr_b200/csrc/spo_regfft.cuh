@@ -238,6 +238,9 @@ struct Axis2Args {
   long long groups;  // host side: lane groups per line set (the launch has groups * blocks_per_group blocks)
   int persistent;    // launch choice: the persistent form (axis2p_kernel) for whole passes
   int balanced;      // launch choice: the balanced form (axis2b_kernel, N2 = 2 N1) for whole passes
+  // The factors in the prime-factor order (axis2pfa_kernel): factor_pfa[k1 + N1 k2] = factor[k(k1, k2)];
+  // null: the two-level kernels with twiddles.
+  const Vec<T>* factor_pfa;
 };
 
 // Dynamic shared memory: (N TB + 2 N) values (axis2_smem).
@@ -689,3 +692,91 @@ __global__ void projection_finalize_kernel(Vec<T>* __restrict__ psi, Vec<T>* __r
 }
 
 }  // namespace spo
+
+namespace spo {
+
+// ---------------------------------------------------------------------------------------------
+// Axis pass for N = N1 N2 with N1, N2 coprime, by the prime-factor (Good-Thomas) mapping: no twiddles
+// between the levels. Point n = (N2 n1 + N1 n2) mod N; the two DFT levels (over n1, then over n2) give
+// X(k1, k2) = DFT_N(x)[k], k = (N2 u k1 + N1 v k2) mod N with u = N2^-1 mod N1, v = N1^-1 mod N2,
+// because exp(-2 pi i n k / N) = exp(-2 pi i n1 k1 / N1) exp(-2 pi i n2 k2 / N2) under these maps. The
+// factor is diagonal in k, so it is applied at (k1, k2) from a table permuted on the host (factor_pfa),
+// and the inverse levels undo the forward ones with the same point map. For r = 48 = 3 x 16 this drops
+// the length-48 twiddles, whose products must be nearly correctly rounded in the mixed form (cmul_comp,
+// ~26 instructions each), and leaves radix 3 (two-part roots) and a power-of-two DFT.
+//   TB batch lanes x LT threads per lane: thread (b, s) takes the first-level lines n2 = s, s + LT, ...
+//   (DFT_N1 each) and, for s < N1, the second-level line k1 = s (DFT_N2, factor, IDFT_N2).
+// Dynamic shared memory: N TB values (the tile) and the factors (mixed form: their parts, see fmul_t).
+// ---------------------------------------------------------------------------------------------
+constexpr int pfa_inverse(int a, int m) {  // a^-1 mod m (a, m coprime)
+  for (int x = 1; x < m; ++x)
+    if ((a * x) % m == 1) return x;
+  return 1;
+}
+template <typename T, int N1, int N2, int TB, int LT>
+__global__ void __launch_bounds__(TB * LT) axis2pfa_kernel(Axis2Args<T> a) {
+  using V = Vec<T>;
+  constexpr int N = N1 * N2;
+  static_assert(LT >= N1, "every second-level line needs a thread");
+  constexpr int kFParts = sizeof(T) == 4 ? kFactorParts : 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* Y = reinterpret_cast<V*>(smem_raw);  // [n2][k1][b]
+  V* f = Y + N * TB;                       // N factors in (k1, k2) order (then their parts)
+  const int b = threadIdx.x % TB;
+  const int s = threadIdx.x / TB;
+  long long base, stride;
+  bool lane_ok;
+  if (a.blocks_per_group == 0) {
+    const long long i0 = static_cast<long long>(blockIdx.x) * TB;
+    base = static_cast<long long>(blockIdx.y) * N * a.inner + i0 + b;
+    stride = a.inner;
+    lane_ok = i0 + b < a.inner;
+  } else {
+    const int grp = blockIdx.x / a.blocks_per_group;
+    const long long in_group = static_cast<long long>(blockIdx.x - grp * a.blocks_per_group) * TB + b;
+    base = static_cast<long long>(blockIdx.y) * a.outer_stride + grp * a.group_stride + a.lane_offset + in_group;
+    stride = a.line_stride;
+    lane_ok = in_group < a.window;
+  }
+  for (int k = threadIdx.x; k < kFParts * N; k += TB * LT) f[k] = a.factor_pfa[k];
+  __syncthreads();
+  // forward, level 1 (DFT_N1 over n1 for each n2)
+  for (int n2 = s; n2 < N2; n2 += LT) {
+    V x[N1];
+    static_for<0, N1>([&](auto n1) {
+      int n = N2 * SPO_CV(n1) + N1 * n2;
+      n = n >= N ? n - N : n;
+      x[n1] = lane_ok ? a.data[base + static_cast<long long>(n) * stride] : cmake<V>(0, 0);
+    });
+    rdft<N1, -1>(x);
+    static_for<0, N1>([&](auto k1) { Y[(n2 * N1 + k1) * TB + b] = x[k1]; });
+  }
+  __syncthreads();
+  // level 2: DFT_N2 over n2, the factor at (k1, k2), inverse DFT_N2
+  if (s < N1) {
+    const int k1 = s;
+    V y[N2];
+    static_for<0, N2>([&](auto n2) { y[n2] = Y[(SPO_CV(n2) * N1 + k1) * TB + b]; });
+    rdft<N2, -1>(y);
+    static_for<0, N2>([&](auto k2) { y[k2] = fmul_t(y[k2], f, N, k1 + N1 * SPO_CV(k2)); });
+    rdft<N2, +1>(y);
+    static_for<0, N2>([&](auto n2) { Y[(SPO_CV(n2) * N1 + k1) * TB + b] = y[n2]; });
+  }
+  __syncthreads();
+  // inverse level 1, store
+  if (lane_ok) {
+    for (int n2 = s; n2 < N2; n2 += LT) {
+      V x[N1];
+      static_for<0, N1>([&](auto k1) { x[k1] = Y[(n2 * N1 + k1) * TB + b]; });
+      rdft<N1, +1>(x);
+      static_for<0, N1>([&](auto n1) {
+        int n = N2 * SPO_CV(n1) + N1 * n2;
+        n = n >= N ? n - N : n;
+        a.data[base + static_cast<long long>(n) * stride] = x[n1];
+      });
+    }
+  }
+}
+
+}  // namespace spo
+

@@ -6,7 +6,7 @@ compiled from its sources), with the reference GPU tests' LCG wave packet over t
 (tests/cuda/cuda_test_setup.hpp:53-64 of the reference), and propagated by the reference's CpuBackend for one
 analysis step (5 time steps). The same case bundle and packet then go through the C ABI:
   - nX = nY = 16 is the benchmark's grid itself: the FP64 form runs the kernels the FP64 line times
-    (axis2b<128>, axis2<48>, xy2p<16>, potential4<32,16>), the mixed form those of the headline
+    (axis2b<128>, axis2pfa<48=3x16>, xy2p<16>, potential4<32,16>), the mixed form those of the headline
     (potential5<32,16> with exp(i A) rows through L2);
   - nX = nY = 4 runs the same Z, r and potential kernels on a smaller (x, y) grid.
 Bars: the FP64 bar (relative L2 1e-10) and the mixed form's 3e-5, on psi and chi.

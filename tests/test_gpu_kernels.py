@@ -277,6 +277,36 @@ def test_balanced_axis_kernel_agrees(nz, nr, precision, monkeypatch):
     assert rel_err(out[1][0], out[0][0]) < tol and rel_err(out[1][1], out[0][1]) < tol
 
 
+@pytest.mark.parametrize("nz,nr", [(48, 40), (56, 24), (80, 112)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_prime_factor_axis_kernel_agrees(nz, nr, precision, monkeypatch):
+    """The prime-factor axis kernel (N = N1 N2 with N1, N2 coprime: 24 = 3 x 8, 40 = 5 x 8, 48 = 3 x 16,
+    56 = 7 x 8, 80 = 5 x 16, 112 = 7 x 16; no twiddles, the factors in the permuted order) against the
+    two-level kernel with twiddles (SPO_B200_PFA=0) over an analysis step: the same wave packet to rounding
+    (1e-12 FP64, 1e-5 mixed)."""
+    from spo_b200 import workload
+    case = workload.config_case({"nz": nz, "nr": nr, "nx": 4, "ny": 4, "j_max": 3, "mj_max": 3,
+                                 "nz_specular": 2 * nz, "nz_potential": nz // 2})
+    rng = np.random.default_rng(43)
+    psi0 = rng.standard_normal(case.psi_shape) + 1j * rng.standard_normal(case.psi_shape)
+    chi0 = rng.standard_normal(case.chi_shape) + 1j * rng.standard_normal(case.chi_shape)
+    out = []
+    for pfa in ("0", "1"):
+        monkeypatch.setenv("SPO_B200_PFA", pfa)
+        be = make(case, "v4", precision)
+        desc = be.describe()
+        if pfa == "1":
+            assert f"z=axis2pfa<{nz}=" in desc and f"r=axis2pfa<{nr}=" in desc, desc
+        else:
+            assert "axis2pfa" not in desc, desc
+        be.read_wave_packet(psi0, chi0)
+        be.propagate_analysis_step()
+        out.append(be.wave_packet_on_host())
+        be.close()
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert rel_l2(out[1][0], out[0][0]) < tol and rel_l2(out[1][1], out[0][1]) < tol
+
+
 @pytest.mark.parametrize("j_max", [11, 13])
 def test_potential5_pads_theta_12_and_14(j_max):
     """The angular grids of the ensemble workload, theta 12 x phi 24 (JMax 11) and theta 14 x phi 28
