@@ -290,10 +290,11 @@ ENSEMBLE_SHAPES = [
 
 
 # DRAM bytes per algorithmic byte of the mixed-form potential kernel (potential5), from one ncu capture of
-# the small case (nX = nY = 8): dram__bytes_read.sum + dram__bytes_write.sum = 1.586 + 0.500 GB against
-# 2.114 GB algorithmic (interaction-region psi read and written once, the exp(i A) table read once). The
-# traffic grows with the columns processed, so the ratio carries over to configuration 3.
-POTENTIAL_DRAM_PER_ALGORITHMIC = (1.586e9 + 0.4998e9) / 2.114e9
+# the small case (nX = nY = 8; profiles/potential5_small_nx8.md): dram__bytes_read.sum + dram__bytes_write.sum
+# = 1.852 + 0.507 GB against 2.378 GB algorithmic (interaction-region psi read and written once, the exp(i A)
+# table read once with its 2-byte modulus corrections). The traffic grows with the columns processed, so the
+# ratio carries over to configuration 3.
+POTENTIAL_DRAM_PER_ALGORITHMIC = (1.852132e9 + 0.506512e9) / 2.378170368e9
 
 
 def run_ensemble(args):
@@ -432,7 +433,7 @@ def main():
                          "traffic": top["bytes_per_launch"] * POTENTIAL_DRAM_PER_ALGORITHMIC
                          if top["name"] == "potential" else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one potential5 launch "
-                                           "on the small case (nX = nY = 8: 2.086 GB for 2.114 GB algorithmic), "
+                                           "on the small case (nX = nY = 8: 2.359 GB for 2.378 GB algorithmic), "
                                            "scaled to this launch by the columns processed",
                          "bytes_per_launch": top["bytes_per_launch"], "avg_launch_ms": avg_ms,
                          "share_of_kernel_time": top["ms"] / total_kernel_ms},

@@ -1193,7 +1193,10 @@ class Step final : public StepBase {
   void interaction() {
     if (s_.nzp == 0) return;
     prof_.begin(stream_);
-    const double bytes = sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia()));
+    // psi of the interaction region read and written, the exp(i A) table read (the mixed form's entries with
+    // their 2-byte modulus corrections)
+    const double bytes = sizeof(V) * (2.0 * s_.nzp * s_.nr * s_.n_xy() * s_.n_rot + static_cast<double>(s_.n_expia())) +
+                         (sizeof(T) == 4 ? 2.0 * static_cast<double>(s_.n_expia()) : 0.0);
     const unsigned points = static_cast<unsigned>(s_.nzp) * s_.nr;
     if (pot_kind_ >= 3) {
       if (pot_kind_ == 6) {
